@@ -1,0 +1,800 @@
+// solver.cu -- tabu-search state on the device and the host step loop.
+//
+// Replaces tabu_search (src/mdp/GPU-MDP-CSR.cu:611-693) and
+// perturbationBasedTabuSearch (src/maxbisection/GPU-MAXBS-CSR.cu:401-512): their
+// host-side init (initialSolution / calculateVertexGain / computeGainsFromScratch,
+// GPU-MDP-CSR.cu:479-519, GPU-MAXBS-CSR.cu:197-219,307-324) runs here as device
+// kernels, and the per-iteration host loop (4-5 launches + a blocking 8-byte D2H
+// per iteration) becomes back-to-back launches of one iteration kernel whose
+// state lives in HBM (sweep.cuh).  The host only touches the device between
+// batches of iterations.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "sweep.cuh"
+#include "ts_host.h"
+
+namespace tsb {
+
+// glibc's rand() after srand(seed): random_r over the 128-byte TYPE_3 state,
+// the generator the MDP start uses (GPU-MDP-CSR.cu:777, seeded at :1248),
+// kept private so the library never touches the process-wide rand() state.
+struct GlibcRand {
+  struct random_data rd;
+  char state[128];
+  explicit GlibcRand(unsigned seed) {
+    std::memset(&rd, 0, sizeof(rd));
+    std::memset(state, 0, sizeof(state));
+    initstate_r(seed, state, sizeof(state), &rd);
+  }
+  int next() {
+    int32_t r = 0;
+    random_r(&rd, &r);
+    return r;
+  }
+};
+
+namespace {
+
+constexpr int kInitTPB = 256;
+
+inline int grid_for(int64_t n, int tpb = kInitTPB) {
+  int64_t b = (n + tpb - 1) / tpb;
+  if (b < 1) b = 1;
+  if (b > 148 * 32) b = 148 * 32;
+  return (int)b;
+}
+
+template <class KeyT>
+__global__ void k_init_mdp(const DevGraph g, const DevSolver<KeyT> s, unsigned long long* obj2) {
+  // calculateVertexGain (GPU-MDP-CSR.cu:502-519): vg[z] += w for z in N(S).
+  for (int32_t i = blockIdx.x; i < s.m; i += gridDim.x) {
+    const int32_t u = s.sol_in[i];
+    unsigned long long acc = 0;
+    for (long long k = g.rowptr[u] + threadIdx.x; k < g.rowptr[u + 1]; k += blockDim.x) {
+      const int2 e = g.adj[k];
+      const int32_t p = s.pos[e.x];
+      atomic_add_key(vg_at(s, p), (KeyT)e.y);
+      if (p < s.m) acc += (unsigned long long)(long long)e.y;
+    }
+    if (acc) atomicAdd(obj2, acc);
+  }
+}
+
+template <class KeyT>
+__global__ void k_init_maxbs(const DevGraph g, const DevSolver<KeyT> s, unsigned long long* cut) {
+  // computeGainsFromScratch / computeFitnessFromScratch (GPU-MAXBS-CSR.cu:197-219).
+  for (int32_t z = blockIdx.x * blockDim.x + threadIdx.x; z < s.n; z += gridDim.x * blockDim.x) {
+    const int32_t pz = s.pos[z];
+    const bool side = pz < s.m;
+    long long same = 0, opp = 0;
+    unsigned long long c = 0;
+    for (long long k = g.rowptr[z]; k < g.rowptr[z + 1]; k++) {
+      const int2 e = g.adj[k];
+      const bool sy = s.pos[e.x] < s.m;
+      if (sy == side) same += e.y;
+      else {
+        opp += e.y;
+        if (e.x > z) c += (unsigned long long)(long long)e.y;
+      }
+    }
+    *vg_at(s, pz) = (KeyT)(same - opp);
+    if (c) atomicAdd(cut, c);
+  }
+}
+
+// W[i][j] = w(sol_in[i], sol_out[j]) (calculateEdgeGain, GPU-MDP-WSwap.cu:607-626),
+// first entry of a duplicated pair.
+template <class KeyT>
+__global__ void k_init_wswap(const DevGraph g, const DevSolver<KeyT> s) {
+  for (int32_t i = blockIdx.x; i < s.m; i += gridDim.x) {
+    const int32_t u = s.sol_in[i];
+    const long long a0 = g.rowptr[u];
+    for (long long k = a0 + threadIdx.x; k < g.rowptr[u + 1]; k += blockDim.x) {
+      const int2 e = g.adj[k];
+      if (k > a0 && g.adj[k - 1].x == e.x) continue;
+      const int32_t p = s.pos[e.x];
+      if (p >= s.m) s.W[(long long)i * s.ldc + (p - s.m)] = e.y;
+    }
+  }
+}
+
+// Objective of a set / bisection given per-vertex flags (1 = inside / side 0).
+__global__ void k_objective(const DevGraph g, int32_t problem, const uint8_t* in,
+                            unsigned long long* out) {
+  for (int32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < g.n; a += gridDim.x * blockDim.x) {
+    unsigned long long acc = 0;
+    for (long long k = g.rowptr[a]; k < g.rowptr[a + 1]; k++) {
+      const int2 e = g.adj[k];
+      if (problem == P_MDP) {
+        if (in[a] && in[e.x]) acc += (unsigned long long)(long long)e.y;
+      } else if (e.x > a && in[a] != in[e.x]) {
+        acc += (unsigned long long)(long long)e.y;
+      }
+    }
+    if (acc) atomicAdd(out, acc);
+  }
+}
+
+template <int PROB, int ST, class KeyT>
+cudaError_t launch_iter(const DevGraph& g, const DevSolver<KeyT>& s, int grid, size_t smem,
+                        cudaStream_t st, int count) {
+  auto fn = iter_kernel<PROB, ST, KeyT>;
+  static bool attr_done = false;  // per instantiation
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  for (int i = 0; i < count; i++) fn<<<grid, kSweepTPB, smem, st>>>(g, s);
+  return cudaGetLastError();
+}
+
+template <int PROB, class KeyT>
+cudaError_t launch_iter_st(int kind, const DevGraph& g, const DevSolver<KeyT>& s, int grid,
+                           size_t smem, cudaStream_t st, int count) {
+  switch (kind) {
+    case S_CSR: return launch_iter<PROB, S_CSR, KeyT>(g, s, grid, smem, st, count);
+    case S_HASH: return launch_iter<PROB, S_HASH, KeyT>(g, s, grid, smem, st, count);
+    case S_WSWAP: return launch_iter<PROB, S_WSWAP, KeyT>(g, s, grid, smem, st, count);
+    case S_BITSET: return launch_iter<PROB, S_BITSET, KeyT>(g, s, grid, smem, st, count);
+    case S_BB: return launch_iter<PROB, S_BB, KeyT>(g, s, grid, smem, st, count);
+    default: return launch_iter<PROB, S_BITSET_BB, KeyT>(g, s, grid, smem, st, count);
+  }
+}
+
+int rows_per_tile(int kind) {
+  switch (kind) {
+    case S_CSR: return Rows<S_CSR>::R;
+    case S_BITSET: return Rows<S_BITSET>::R;
+    case S_BITSET_BB: return Rows<S_BITSET_BB>::R;
+    default: return Rows<S_HASH>::R;
+  }
+}
+
+}  // namespace
+}  // namespace tsb
+
+using namespace tsb;
+
+struct ts_solver {
+  ts_graph* g = nullptr;
+  ts_params p{};
+  bool wide = false;
+  int32_t n = 0, m = 0, delta = 0, ldc = 0;
+  int64_t P = 0;
+  int R = 0;
+  int32_t n_row_blocks = 0, n_chunks = 0, chunk_cols = 0, stage_bytes = 0;
+  size_t dyn_smem = 0;
+  int grid = 0;
+  int32_t num_pert = 1;
+  int64_t log_cap = 0, trace_cap = 0;
+  int64_t window_events = 0;
+  DevBuf sol_in, sol_out, vg_in, vg_out, tab_in, tab_out, pos, W, st, recs, movelog, trace, draws;
+  std::mt19937 rng;
+  std::vector<long long> host_draws;  // every perturbation event drawn so far, k draws each
+  int64_t events_drawn = 0;
+  bool initialized = false;
+  int64_t admitted_target = 0;
+  DevState* h_st = nullptr;  // pinned mirror
+
+  template <class KeyT>
+  DevSolver<KeyT> dev() const {
+    DevSolver<KeyT> s;
+    std::memset(&s, 0, sizeof(s));
+    s.n = n; s.m = m; s.delta = delta; s.ldc = ldc;
+    s.problem = p.problem;
+    s.tenure_policy = p.tenure_policy;
+    s.tenure = p.tenure;
+    s.maxt = p.maxt;
+    s.piter = p.piter;
+    s.num_pert = num_pert;
+    const int c1s[4] = {15, 30, 60, 120};
+    for (int i = 0; i < 4; i++) s.c2_tab[i] = (int32_t)round(0.7 * c1s[i]);  // :664
+    s.c2_fixed = (int32_t)round(0.7 * p.tenure);
+    s.n_row_blocks = n_row_blocks; s.n_chunks = n_chunks; s.chunk_cols = chunk_cols;
+    s.stage_bytes = stage_bytes;
+    s.P = P;
+    s.sol_in = sol_in.as<int32_t>(); s.sol_out = sol_out.as<int32_t>();
+    s.vg_in = vg_in.as<KeyT>(); s.vg_out = vg_out.as<KeyT>();
+    s.tab_in = tab_in.as<int32_t>(); s.tab_out = tab_out.as<int32_t>();
+    s.pos = pos.as<int32_t>();
+    s.W = W.as<int32_t>();
+    s.st = st.as<DevState>();
+    s.recs = recs.as<CtaRec>();
+    s.movelog = movelog.as<int2>();
+    s.log_cap = log_cap;
+    s.trace = p.trace ? trace.as<TraceRec>() : nullptr;
+    s.trace_cap = trace_cap;
+    s.draws = draws.as<long long>();
+    s.draw_events = window_events;
+    return s;
+  }
+};
+
+namespace {
+
+ts_status read_state(ts_solver* s) {
+  TS_CUDA(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(DevState), cudaMemcpyDeviceToHost, s->g->stream));
+  TS_CUDA(cudaStreamSynchronize(s->g->stream));
+  return TS_OK;
+}
+
+ts_status write_state(ts_solver* s) {
+  TS_CUDA(cudaMemcpyAsync(s->st.p, s->h_st, sizeof(DevState), cudaMemcpyHostToDevice, s->g->stream));
+  TS_CUDA(cudaStreamSynchronize(s->g->stream));
+  return TS_OK;
+}
+
+template <class KeyT>
+ts_status launch_batch(ts_solver* s, int count) {
+  DevSolver<KeyT> d = s->dev<KeyT>();
+  DevGraph g = s->g->dev();
+  cudaError_t e = s->p.problem == P_MDP
+                      ? launch_iter_st<P_MDP, KeyT>(s->g->kind, g, d, s->grid, s->dyn_smem, s->g->stream, count)
+                      : launch_iter_st<P_MAXBS, KeyT>(s->g->kind, g, d, s->grid, s->dyn_smem, s->g->stream, count);
+  if (e != cudaSuccess) return cuda_fail(e, "iteration kernel launch");
+  return TS_OK;
+}
+
+// One perturbation event: k distinct flat move indices (GPU-MAXBS-CSR.cu:481-492).
+void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out) {
+  std::unordered_set<long long> used;
+  for (int q = 0; q < k; q++) {
+    long long mv;
+    do {
+      if (P - 1 <= INT32_MAX) {
+        std::uniform_int_distribution<int> d(0, (int)(P - 1));
+        mv = d(rng);
+      } else {  // past the reference's int range (it overflows there)
+        std::uniform_int_distribution<long long> d(0, P - 1);
+        mv = d(rng);
+      }
+    } while (used.count(mv));
+    used.insert(mv);
+    out.push_back(mv);
+  }
+}
+
+void mdp_random_set(int32_t n, int32_t m, uint32_t seed, std::vector<int32_t>& ids) {
+  GlibcRand r(seed);
+  std::vector<uint8_t> used(n, 0);
+  ids.clear();
+  while ((int32_t)ids.size() < m) {
+    int32_t idx = r.next() % n;
+    if (!used[idx]) { used[idx] = 1; ids.push_back(idx); }
+  }
+}
+
+void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0) {
+  std::vector<int> vertices(n);
+  for (int32_t i = 0; i < n; i++) vertices[i] = i;
+  std::shuffle(vertices.begin(), vertices.end(), rng);  // randomPartition :187-195
+  side0.assign(n, 0);
+  for (int32_t i = 0; i < n / 2; i++) side0[vertices[i]] = 1;
+}
+
+// MaxBS: make sure the device window holds the draws of every perturbation
+// event that can happen before `target` (events are at least piter apart).
+ts_status prepare_draws(ts_solver* s, int64_t iters_ahead) {
+  if (s->p.problem != P_MAXBS) return TS_OK;
+  const int64_t consumed = s->h_st->pert_events;
+  int64_t need = iters_ahead / std::max(1, s->p.piter) + 2;
+  if (need > s->window_events) need = s->window_events;
+  const int k = s->num_pert;
+  while (s->events_drawn < consumed + need) {
+    draw_event(s->rng, s->P, k, s->host_draws);
+    s->events_drawn++;
+  }
+  TS_CUDA(cudaMemcpyAsync(s->draws.p, s->host_draws.data() + consumed * k,
+                          sizeof(long long) * need * k, cudaMemcpyHostToDevice, s->g->stream));
+  s->h_st->pert_base = consumed;
+  return TS_OK;
+}
+
+template <class KeyT>
+ts_status init_device(ts_solver* s, const std::vector<uint8_t>& inside) {
+  const int32_t n = s->n, m = s->m;
+  cudaStream_t st = s->g->stream;
+  std::vector<int32_t> sin(m), sout(s->ldc, 0), pos(n);
+  int32_t x = 0, y = 0;
+  for (int32_t v = 0; v < n; v++) {  // initialSolution: ascending ids per side
+    if (inside[v]) { sin[x] = v; pos[v] = x; x++; }
+    else { sout[y] = v; pos[v] = m + y; y++; }
+  }
+  TS_CUDA(cudaMemcpyAsync(s->sol_in.p, sin.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice, st));
+  TS_CUDA(cudaMemcpyAsync(s->sol_out.p, sout.data(), sizeof(int32_t) * s->ldc, cudaMemcpyHostToDevice, st));
+  TS_CUDA(cudaMemcpyAsync(s->pos.p, pos.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  TS_CUDA(cudaMemsetAsync(s->vg_in.p, 0, s->vg_in.bytes, st));
+  TS_CUDA(cudaMemsetAsync(s->vg_out.p, 0, s->vg_out.bytes, st));
+  TS_CUDA(cudaMemsetAsync(s->tab_in.p, 0, s->tab_in.bytes, st));
+  TS_CUDA(cudaMemsetAsync(s->tab_out.p, 0, s->tab_out.bytes, st));
+  DevBuf acc;
+  ts_status rc;
+  if ((rc = acc.alloc(sizeof(unsigned long long), "alloc")) != TS_OK) return rc;
+  TS_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long), st));
+  DevSolver<KeyT> d = s->dev<KeyT>();
+  DevGraph g = s->g->dev();
+  if (s->p.problem == P_MDP) k_init_mdp<KeyT><<<grid_for((int64_t)m * 32), kInitTPB, 0, st>>>(g, d, acc.as<unsigned long long>());
+  else k_init_maxbs<KeyT><<<grid_for(n), kInitTPB, 0, st>>>(g, d, acc.as<unsigned long long>());
+  TS_CUDA(cudaGetLastError());
+  if (s->g->kind == S_WSWAP) {
+    TS_CUDA(cudaMemsetAsync(s->W.p, 0, s->W.bytes, st));
+    k_init_wswap<KeyT><<<grid_for((int64_t)m * 32), kInitTPB, 0, st>>>(g, d);
+    TS_CUDA(cudaGetLastError());
+  }
+  unsigned long long obj = 0;
+  TS_CUDA(cudaMemcpyAsync(&obj, acc.p, sizeof(obj), cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaStreamSynchronize(st));
+  long long objective = (long long)obj;
+  if (s->p.problem == P_MDP) objective /= 2;
+  std::memset(s->h_st, 0, sizeof(DevState));
+  s->h_st->cur = objective;
+  s->h_st->best = objective;
+  return write_state(s);
+}
+
+ts_status objective_of(ts_solver* s, const std::vector<uint8_t>& inside, long long* out) {
+  cudaStream_t st = s->g->stream;
+  DevBuf flags, acc;
+  ts_status rc;
+  if ((rc = flags.alloc(s->n, "alloc")) != TS_OK) return rc;
+  if ((rc = acc.alloc(sizeof(unsigned long long), "alloc")) != TS_OK) return rc;
+  TS_CUDA(cudaMemcpyAsync(flags.p, inside.data(), s->n, cudaMemcpyHostToDevice, st));
+  TS_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long), st));
+  k_objective<<<grid_for(s->n), kInitTPB, 0, st>>>(s->g->dev(), s->p.problem, flags.as<uint8_t>(),
+                                                   acc.as<unsigned long long>());
+  TS_CUDA(cudaGetLastError());
+  unsigned long long v = 0;
+  TS_CUDA(cudaMemcpyAsync(&v, acc.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaStreamSynchronize(st));
+  long long r = (long long)v;
+  if (s->p.problem == P_MDP) r /= 2;
+  *out = r;
+  return TS_OK;
+}
+
+// Current inside set and the best one (by undoing the moves logged after the
+// last improvement; a swap is its own inverse).
+ts_status fetch_sets(ts_solver* s, std::vector<int32_t>& sin, std::vector<int32_t>& sout,
+                     bool best) {
+  cudaStream_t st = s->g->stream;
+  sin.assign(s->m, 0);
+  sout.assign(s->ldc, 0);
+  TS_CUDA(cudaMemcpyAsync(sin.data(), s->sol_in.p, sizeof(int32_t) * s->m, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaMemcpyAsync(sout.data(), s->sol_out.p, sizeof(int32_t) * s->ldc, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaStreamSynchronize(st));
+  if (best) {
+    const int64_t from = s->h_st->best_log_n, to = std::min<int64_t>(s->h_st->log_n, s->log_cap);
+    if (to > from) {
+      std::vector<int2> tail(to - from);
+      TS_CUDA(cudaMemcpyAsync(tail.data(), s->movelog.as<int2>() + from, sizeof(int2) * (to - from),
+                              cudaMemcpyDeviceToHost, st));
+      TS_CUDA(cudaStreamSynchronize(st));
+      for (int64_t k = (int64_t)tail.size() - 1; k >= 0; k--) std::swap(sin[tail[k].x], sout[tail[k].y]);
+    }
+  }
+  return TS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ts_status ts_params_default(int32_t problem, ts_params* out) {
+  if (!out || (problem != TS_PROBLEM_MDP && problem != TS_PROBLEM_MAXBS)) {
+    set_error("ts_params_default: bad argument");
+    return TS_ERR_INVALID_ARG;
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->problem = problem;
+  if (problem == TS_PROBLEM_MDP) {
+    out->m = 100;                 // 'sparse' data set, GPU-MDP-CSR.cu:306
+    out->max_iter = 50000;        // :55
+    out->tenure_policy = TS_TENURE_REF;
+    out->tenure = 15;
+  } else {
+    out->max_iter = 1000000;      // MacutParams, GPU-MAXBS-CSR.cu:71
+    out->tenure_policy = TS_TENURE_REF;
+    out->tenure = 25;
+  }
+  out->maxt = 200;
+  out->piter = 500;
+  out->gamma = 150;
+  out->seed = 1;
+  return TS_OK;
+}
+
+ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
+  if (!out) { set_error("ts_solver_create: out is NULL"); return TS_ERR_INVALID_ARG; }
+  *out = nullptr;
+  if (!g || !p) { set_error("ts_solver_create: NULL argument"); return TS_ERR_INVALID_ARG; }
+  if (p->problem != TS_PROBLEM_MDP && p->problem != TS_PROBLEM_MAXBS) {
+    set_error("ts_solver_create: unknown problem");
+    return TS_ERR_INVALID_ARG;
+  }
+  const int32_t n = g->n;
+  const int32_t m = p->problem == TS_PROBLEM_MDP ? p->m : n / 2;
+  if (m < 1 || m >= n) { set_error("ts_solver_create: need 1 <= m < n"); return TS_ERR_INVALID_ARG; }
+  if (p->max_iter < 0 || p->piter < 1 || p->gamma < 0 || p->maxt < 1 ||
+      (p->tenure_policy != TS_TENURE_REF && p->tenure_policy != TS_TENURE_FIXED) || p->tenure < 0) {
+    set_error("ts_solver_create: bad parameters");
+    return TS_ERR_INVALID_ARG;
+  }
+  TS_CUDA(cudaSetDevice(g->device));
+  auto* s = new ts_solver;
+  s->g = g;
+  s->p = *p;
+  s->n = n;
+  s->m = m;
+  s->delta = n - m;
+  s->ldc = (s->delta + 3) & ~3;
+  s->P = (int64_t)m * s->delta;
+  // 32-bit pair keys while every gain stays within +-2^30.
+  s->wide = 4 * g->max_wdeg >= (1LL << 30);
+  s->R = rows_per_tile(g->kind);
+  s->n_row_blocks = (m + s->R - 1) / s->R;
+  int64_t want_chunks = (4 * 148 + s->n_row_blocks - 1) / s->n_row_blocks;
+  int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
+  cols = ((cols + kPassCols - 1) / kPassCols) * kPassCols;
+  if (cols < kPassCols) cols = kPassCols;
+  if (cols > 8 * kPassCols) cols = 8 * kPassCols;
+  s->chunk_cols = (int32_t)cols;
+  s->n_chunks = (int32_t)((s->delta + cols - 1) / cols);
+  s->grid = s->n_row_blocks * s->n_chunks;
+  if (g->kind == S_CSR) {
+    s->stage_bytes = 0;
+    s->dyn_smem = sizeof(uint32_t) * (size_t)s->chunk_cols;
+  } else if (g->kind == S_WSWAP) {
+    s->stage_bytes = 0;
+    s->dyn_smem = 16;
+  } else if (g->kind == S_BITSET || g->kind == S_BITSET_BB) {
+    int64_t b = (int64_t)s->R * g->wpr * 8;
+    s->stage_bytes = (int32_t)std::min<int64_t>(b, 192 * 1024);
+    s->dyn_smem = s->stage_bytes;
+  } else {
+    s->stage_bytes = 64 * 1024;
+    s->dyn_smem = s->stage_bytes;
+  }
+  const int32_t g_eff = std::min(p->gamma, n);
+  s->num_pert = std::max(1, g_eff / 2);  // GPU-MAXBS-CSR.cu:433-434
+  int64_t pert_moves = p->problem == TS_PROBLEM_MAXBS ? (p->max_iter / p->piter + 1) * s->num_pert : 0;
+  s->log_cap = p->max_iter + pert_moves + 1;
+  s->trace_cap = p->trace ? p->max_iter + pert_moves + 2 : 0;
+  s->window_events = p->problem == TS_PROBLEM_MAXBS ? 64 : 1;
+  const size_t kb = s->wide ? sizeof(long long) : sizeof(int32_t);
+  ts_status rc = TS_OK;
+  auto A = [&](DevBuf& b, size_t bytes, const char* what) {
+    if (rc == TS_OK) rc = b.alloc(bytes, what);
+  };
+  A(s->sol_in, sizeof(int32_t) * (size_t)m, "alloc sol_in");
+  A(s->sol_out, sizeof(int32_t) * (size_t)s->ldc, "alloc sol_out");
+  A(s->vg_in, kb * (size_t)m, "alloc vg_in");
+  A(s->vg_out, kb * (size_t)s->ldc, "alloc vg_out");
+  A(s->tab_in, sizeof(int32_t) * (size_t)m, "alloc tab_in");
+  A(s->tab_out, sizeof(int32_t) * (size_t)s->ldc, "alloc tab_out");
+  A(s->pos, sizeof(int32_t) * (size_t)n, "alloc pos");
+  A(s->st, sizeof(DevState), "alloc state");
+  A(s->recs, sizeof(CtaRec) * (size_t)s->grid, "alloc records");
+  A(s->movelog, sizeof(int2) * (size_t)s->log_cap, "alloc move log");
+  if (p->trace) A(s->trace, sizeof(TraceRec) * (size_t)s->trace_cap, "alloc trace");
+  A(s->draws, sizeof(long long) * (size_t)(s->window_events * s->num_pert), "alloc draws");
+  if (g->kind == S_WSWAP) {
+    // Padded to whole row blocks so a tile never reads past the matrix.
+    size_t rows = (size_t)s->n_row_blocks * s->R;
+    A(s->W, sizeof(int32_t) * rows * (size_t)s->ldc, "alloc WSwap matrix");
+  }
+  if (rc == TS_OK) {
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&s->h_st), sizeof(DevState));
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMallocHost state");
+  }
+  if (rc != TS_OK) { delete s; return rc; }
+  std::memset(s->h_st, 0, sizeof(DevState));
+  *out = s;
+  return TS_OK;
+}
+
+ts_status ts_solver_init(ts_solver* s, const int32_t* initial) {
+  if (!s) { set_error("ts_solver_init: NULL solver"); return TS_ERR_INVALID_ARG; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  const int32_t n = s->n, m = s->m;
+  std::vector<uint8_t> inside(n, 0);
+  s->rng.seed(s->p.seed);
+  s->host_draws.clear();
+  s->events_drawn = 0;
+  if (s->p.problem == P_MDP) {
+    if (!initial) {
+      std::vector<int32_t> ids;
+      mdp_random_set(n, m, s->p.seed, ids);
+      for (int32_t v : ids) inside[v] = 1;
+    } else {
+      for (int32_t i = 0; i < m; i++) {
+        int32_t v = initial[i];
+        if (v < 0 || v >= n || inside[v]) {
+          set_error("ts_solver_init: MDP initial set must hold m distinct ids in [0, n)");
+          return TS_ERR_INVALID_ARG;
+        }
+        inside[v] = 1;
+      }
+    }
+  } else {
+    if (!initial) {
+      maxbs_random_part(s->rng, n, inside);
+    } else {
+      int32_t zeros = 0;
+      for (int32_t v = 0; v < n; v++) {
+        if (initial[v] != 0 && initial[v] != 1) {
+          set_error("ts_solver_init: MaxBS partition entries must be 0 or 1");
+          return TS_ERR_INVALID_ARG;
+        }
+        inside[v] = initial[v] == 0;
+        zeros += inside[v];
+      }
+      if (zeros != m) {
+        set_error("ts_solver_init: MaxBS partition must put floor(n/2) vertices in part 0");
+        return TS_ERR_INVALID_ARG;
+      }
+    }
+  }
+  ts_status rc = s->wide ? init_device<long long>(s, inside) : init_device<int32_t>(s, inside);
+  if (rc != TS_OK) return rc;
+  s->initialized = true;
+  return TS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Admits up to k iterations: target = iter + k (bounded by max_iter and, for
+// MaxBS, by the perturbation-draw window), draws staged, state written.
+// Requires a synchronised state mirror (read_state).
+ts_status prepare_batch(ts_solver* s, int64_t k, int64_t* admitted) {
+  *admitted = 0;
+  if (s->h_st->done) return TS_OK;
+  int64_t sub = std::min<int64_t>(k, s->p.max_iter - s->h_st->iter);
+  if (sub < 0) sub = 0;
+  if (s->p.problem == P_MAXBS) {
+    // A batch may meet at most window_events - 2 perturbation events.
+    sub = std::min<int64_t>(sub, (s->window_events - 2) * (int64_t)s->p.piter);
+  }
+  s->h_st->target = s->h_st->iter + sub;
+  ts_status rc;
+  if ((rc = prepare_draws(s, sub)) != TS_OK) return rc;
+  if ((rc = write_state(s)) != TS_OK) return rc;
+  s->admitted_target = s->h_st->target;
+  *admitted = sub;
+  return TS_OK;
+}
+
+ts_status enqueue_launches(ts_solver* s, int64_t launches) {
+  while (launches > 0) {
+    int c = (int)std::min<int64_t>(launches, 1 << 20);
+    ts_status rc = s->wide ? launch_batch<long long>(s, c) : launch_batch<int32_t>(s, c);
+    if (rc != TS_OK) return rc;
+    launches -= c;
+  }
+  return TS_OK;
+}
+
+// Waits for the admitted batch; tops it up when exact passes consumed launches.
+ts_status finish_batch(ts_solver* s) {
+  ts_status rc;
+  for (int guard = 0; guard < 1 << 20; guard++) {
+    if ((rc = read_state(s)) != TS_OK) return rc;
+    if (s->h_st->err) {
+      set_error("device error word set (" + std::to_string(s->h_st->err) + ")");
+      return TS_ERR_DEVICE;
+    }
+    if (s->h_st->done || s->h_st->iter >= s->admitted_target) return TS_OK;
+    if ((rc = enqueue_launches(s, s->admitted_target - s->h_st->iter + 1)) != TS_OK) return rc;
+  }
+  set_error("no progress");
+  return TS_ERR_DEVICE;
+}
+
+}  // namespace
+
+extern "C" {
+
+ts_status ts_solver_step(ts_solver* s, int64_t k, int64_t* done_iters) {
+  if (done_iters) *done_iters = 0;
+  if (!s) { set_error("ts_solver_step: NULL solver"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_step: call ts_solver_init first"); return TS_ERR_STATE; }
+  if (k < 0) { set_error("ts_solver_step: negative k"); return TS_ERR_INVALID_ARG; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = read_state(s);
+  if (rc != TS_OK) return rc;
+  const int64_t start = s->h_st->iter;
+  int64_t remaining = k;
+  while (remaining > 0 && !s->h_st->done && s->h_st->iter < s->p.max_iter) {
+    int64_t sub = 0;
+    if ((rc = prepare_batch(s, remaining, &sub)) != TS_OK) return rc;
+    if (sub <= 0) break;
+    const int64_t iter0 = s->h_st->iter;
+    if ((rc = enqueue_launches(s, sub)) != TS_OK) return rc;
+    if ((rc = finish_batch(s)) != TS_OK) return rc;
+    remaining -= s->h_st->iter - iter0;
+  }
+  if (done_iters) *done_iters = s->h_st->iter - start;
+  return TS_OK;
+}
+
+ts_status ts_solver_prepare(ts_solver* s, int64_t k, int64_t* prepared) {
+  if (prepared) *prepared = 0;
+  if (!s) { set_error("ts_solver_prepare: NULL solver"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_prepare: call ts_solver_init first"); return TS_ERR_STATE; }
+  if (k < 0) { set_error("ts_solver_prepare: negative k"); return TS_ERR_INVALID_ARG; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = read_state(s);
+  if (rc != TS_OK) return rc;
+  int64_t sub = 0;
+  if ((rc = prepare_batch(s, k, &sub)) != TS_OK) return rc;
+  if (prepared) *prepared = sub;
+  return TS_OK;
+}
+
+ts_status ts_solver_enqueue(ts_solver* s, int64_t k) {
+  if (!s || k < 0) { set_error("ts_solver_enqueue: bad argument"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_enqueue: call ts_solver_init first"); return TS_ERR_STATE; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  return enqueue_launches(s, k);
+}
+
+ts_status ts_solver_sync(ts_solver* s, int64_t* iter) {
+  if (iter) *iter = 0;
+  if (!s) { set_error("ts_solver_sync: NULL solver"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_sync: call ts_solver_init first"); return TS_ERR_STATE; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = finish_batch(s);
+  if (rc != TS_OK) return rc;
+  if (iter) *iter = s->h_st->iter;
+  return TS_OK;
+}
+
+ts_status ts_solver_result(ts_solver* s, ts_result* out, int32_t* best_sol) {
+  if (!s || !out) { set_error("ts_solver_result: NULL argument"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_result: call ts_solver_init first"); return TS_ERR_STATE; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = read_state(s);
+  if (rc != TS_OK) return rc;
+  std::vector<int32_t> sin, sout;
+  if ((rc = fetch_sets(s, sin, sout, true)) != TS_OK) return rc;
+  std::vector<uint8_t> inside(s->n, 0);
+  for (int32_t v : sin) inside[v] = 1;
+  long long bt = 0;
+  if ((rc = objective_of(s, inside, &bt)) != TS_OK) return rc;
+  std::memset(out, 0, sizeof(*out));
+  out->iterations = s->h_st->iter;
+  out->evaluations = s->h_st->evaluations;
+  out->cur = s->h_st->cur;
+  out->best = s->h_st->best;
+  out->best_true = bt;
+  out->perturbations = s->h_st->pert_moves;
+  out->stopped = s->h_st->stopped;
+  out->m = s->m;
+  out->n = s->n;
+  out->device_error = s->h_st->err;
+  if (best_sol) {
+    if (s->p.problem == P_MDP) {
+      std::memcpy(best_sol, sin.data(), sizeof(int32_t) * s->m);
+    } else {
+      for (int32_t v = 0; v < s->n; v++) best_sol[v] = inside[v] ? 0 : 1;
+    }
+  }
+  return TS_OK;
+}
+
+ts_status ts_solver_state(ts_solver* s, int32_t* sol, int32_t* pos, int32_t* tab, int64_t* vg) {
+  if (!s) { set_error("ts_solver_state: NULL solver"); return TS_ERR_INVALID_ARG; }
+  if (!s->initialized) { set_error("ts_solver_state: call ts_solver_init first"); return TS_ERR_STATE; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  cudaStream_t st = s->g->stream;
+  const int32_t n = s->n, m = s->m, d = s->delta;
+  std::vector<int32_t> sin(m), sout(s->ldc), tin(m), tout(s->ldc), p(n);
+  std::vector<long long> vin(m), vout(s->ldc);
+  TS_CUDA(cudaMemcpyAsync(sin.data(), s->sol_in.p, 4 * (size_t)m, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaMemcpyAsync(sout.data(), s->sol_out.p, 4 * (size_t)s->ldc, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaMemcpyAsync(tin.data(), s->tab_in.p, 4 * (size_t)m, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaMemcpyAsync(tout.data(), s->tab_out.p, 4 * (size_t)s->ldc, cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaMemcpyAsync(p.data(), s->pos.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  if (s->wide) {
+    TS_CUDA(cudaMemcpyAsync(vin.data(), s->vg_in.p, 8 * (size_t)m, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaMemcpyAsync(vout.data(), s->vg_out.p, 8 * (size_t)s->ldc, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
+  } else {
+    std::vector<int32_t> a(m), b(s->ldc);
+    TS_CUDA(cudaMemcpyAsync(a.data(), s->vg_in.p, 4 * (size_t)m, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaMemcpyAsync(b.data(), s->vg_out.p, 4 * (size_t)s->ldc, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
+    for (int32_t i = 0; i < m; i++) vin[i] = a[i];
+    for (int32_t j = 0; j < s->ldc; j++) vout[j] = b[j];
+  }
+  for (int32_t i = 0; i < m; i++) {
+    if (sol) sol[i] = sin[i];
+    if (tab) tab[sin[i]] = tin[i];
+    if (vg) vg[sin[i]] = vin[i];
+  }
+  for (int32_t j = 0; j < d; j++) {
+    if (sol) sol[m + j] = sout[j];
+    if (tab) tab[sout[j]] = tout[j];
+    if (vg) vg[sout[j]] = vout[j];
+  }
+  if (pos) std::memcpy(pos, p.data(), 4 * (size_t)n);
+  return TS_OK;
+}
+
+ts_status ts_solver_trace(ts_solver* s, ts_trace_rec* out, int64_t cap, int64_t* n_out) {
+  if (!s || (cap > 0 && !out)) { set_error("ts_solver_trace: bad argument"); return TS_ERR_INVALID_ARG; }
+  if (n_out) *n_out = 0;
+  if (!s->p.trace) { set_error("ts_solver_trace: solver created without trace"); return TS_ERR_STATE; }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = read_state(s);
+  if (rc != TS_OK) return rc;
+  int64_t have = std::min<int64_t>(s->h_st->trace_n, s->trace_cap);
+  int64_t cnt = std::min<int64_t>(have, cap);
+  static_assert(sizeof(ts_trace_rec) == sizeof(TraceRec), "trace record layout");
+  if (cnt > 0) {
+    TS_CUDA(cudaMemcpyAsync(out, s->trace.p, sizeof(TraceRec) * cnt, cudaMemcpyDeviceToHost, s->g->stream));
+    TS_CUDA(cudaStreamSynchronize(s->g->stream));
+  }
+  if (n_out) *n_out = have;
+  return TS_OK;
+}
+
+ts_status ts_random_start(int32_t problem, int32_t n, int32_t m, uint32_t seed, int32_t* out) {
+  if (!out || n < 2 || (problem == TS_PROBLEM_MDP && (m < 1 || m >= n)) ||
+      (problem != TS_PROBLEM_MDP && problem != TS_PROBLEM_MAXBS)) {
+    set_error("ts_random_start: bad argument");
+    return TS_ERR_INVALID_ARG;
+  }
+  if (problem == TS_PROBLEM_MDP) {
+    std::vector<int32_t> ids;
+    mdp_random_set(n, m, seed, ids);
+    std::memcpy(out, ids.data(), sizeof(int32_t) * m);
+  } else {
+    std::mt19937 rng;
+    rng.seed(seed);
+    std::vector<uint8_t> side0;
+    maxbs_random_part(rng, n, side0);
+    for (int32_t v = 0; v < n; v++) out[v] = side0[v] ? 0 : 1;
+  }
+  return TS_OK;
+}
+
+ts_status ts_perturb_draws(int32_t n, uint32_t seed, int32_t gamma, int32_t init_random,
+                           int32_t n_events, int64_t* out) {
+  if (!out || n < 2 || n_events < 0 || gamma < 0) {
+    set_error("ts_perturb_draws: bad argument");
+    return TS_ERR_INVALID_ARG;
+  }
+  std::mt19937 rng;
+  rng.seed(seed);
+  if (init_random) {
+    std::vector<uint8_t> side0;
+    maxbs_random_part(rng, n, side0);
+  }
+  const int k = std::max(1, std::min(gamma, n) / 2);
+  const int64_t m = n / 2, P = m * (int64_t)(n - m);
+  std::vector<long long> d;
+  for (int32_t e = 0; e < n_events; e++) draw_event(rng, P, k, d);
+  for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
+  return TS_OK;
+}
+
+ts_status ts_solver_destroy(ts_solver* s) {
+  if (!s) return TS_OK;
+  cudaSetDevice(s->g->device);
+  cudaStreamSynchronize(s->g->stream);
+  if (s->h_st) cudaFreeHost(s->h_st);
+  delete s;
+  return TS_OK;
+}
+
+}  // extern "C"

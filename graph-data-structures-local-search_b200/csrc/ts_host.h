@@ -1,0 +1,88 @@
+// ts_host.h -- host-side objects behind the C-ABI handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ts_b200.h"
+#include "ts_internal.cuh"
+
+namespace tsb {
+
+// Thread-local message of the last failing call.
+void set_error(const std::string& msg);
+const char* last_error();
+
+// Records the failure and returns TS_ERR_CUDA (or TS_ERR_OUT_OF_MEMORY).
+ts_status cuda_fail(cudaError_t e, const char* what);
+
+#define TS_CUDA(call)                                     \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return ::tsb::cuda_fail(e_, #call); \
+  } while (0)
+
+// Owning device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  ts_status alloc(size_t nbytes, const char* what) {
+    release();
+    if (nbytes == 0) nbytes = 16;
+    cudaError_t e = cudaMalloc(&p, nbytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_fail(e, what);
+    }
+    bytes = nbytes;
+    return TS_OK;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace tsb
+
+struct ts_graph {
+  int32_t n = 0;
+  int32_t kind = 0;
+  int32_t drop_self_loops = 0;
+  int32_t device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t num_edges = 0;
+  int64_t entries = 0;
+  int64_t max_wdeg = 0;
+  int64_t wpr = 0;
+  int64_t hash_slots = 0;
+  tsb::DevBuf rowptr, adj, bits, hoff, htab;
+  // Host copy of the CSR row pointers/degrees (for footprint planning and the
+  // solver's staging budgets); small: n+1 int64.
+  std::vector<int64_t> h_rowptr;
+  tsb::DevGraph dev() const {
+    tsb::DevGraph g;
+    g.n = n;
+    g.kind = kind;
+    g.entries = entries;
+    g.rowptr = rowptr.as<int64_t>();
+    g.adj = adj.as<int2>();
+    g.bits = bits.as<uint64_t>();
+    g.wpr = wpr;
+    g.hoff = hoff.as<int64_t>();
+    g.htab = htab.as<int2>();
+    return g;
+  }
+  int64_t device_bytes() const {
+    return (int64_t)(rowptr.bytes + adj.bytes + bits.bytes + hoff.bytes + htab.bytes);
+  }
+};
