@@ -1,0 +1,409 @@
+#!/usr/bin/env python3
+"""Benchmark of the tabu-search hot path on one B200 (per rank).
+
+Workload (default): plain Max Bisection tabu search on the seeded
+conflict-style graph -- n = 100,000 unit-square points joined within a radius
+for mean degree ~60 plus 2,000 cliques of 8-32 vertices, node weights
+U[1,1000], w(u,v) = nw_u + nw_v -- from a seeded balanced random partition,
+tenure 50, Piter 500, gamma 150, with all six lookup structures side by side.
+Every iteration evaluates all floor(n/2)*ceil(n/2) = 2.5e9 swap pairs.
+
+One STEP = one tabu iteration (all-pairs sweep + argmax + move) on each of the
+six structures.  Each iteration is timed on the device with CUDA events on the
+library's stream; a 256 MiB buffer is written between timed iterations so no
+iteration starts with a warm L2.  `value` is swap-gains/s of the whole job
+(pairs evaluated / device time); `e2e` runs the same solves through the C-ABI
+from pinned host edge lists (graph upload and build, start, iterations, result
+read back) under a wall clock.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "graph-data-structures-local-search_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "tabu iters/s & swap-gains/s (frac HBM roof); batched solves/s + p50/p99 vs plain"
+UNIT = "swap-gains/s"
+WORKLOAD = ("config2: plain Max Bisection tabu search, conflict-style graph n=100000 "
+            "(radius for mean degree ~60 + 2000 cliques of 8-32), tenure 50, Piter 500, gamma 150, "
+            "six lookup structures")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, nm in enumerate(names):
+                    if r[4 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+WORKLOADS = {
+    "config2": ("maxbs", WORKLOAD),
+    "config3": ("mdp", "config3: plain MDP, Chung-Lu n=200000 (exponent 2.3, mean degree 50, max 5000), "
+                       "m=2000, tenure 100"),
+    "config1": ("mdp", "config1: plain MDP, Erdos-Renyi n=2000 mean degree 20, m=200, tenure 20"),
+}
+
+
+def build_workload(name: str = "config2"):
+    from ts_b200 import gen
+    wl = getattr(gen, name)()
+    wl["problem"], wl["desc"] = WORKLOADS[name]
+    return wl
+
+
+def algorithmic_bytes(kind: str, n: int, m: int, ldc: int, key_bytes: int, deg_in: np.ndarray,
+                      cap_in: np.ndarray, wpr: int) -> int:
+    """Compulsory HBM bytes of one iteration of `kind` (roofline)."""
+    delta = n - m
+    base = m * (key_bytes + 8) + delta * (key_bytes + 4)  # row side: vg, tabu, id; columns: vg, tabu
+    if kind == "csr":
+        return base + 16 * m + 12 * int(deg_in.sum())  # rowptr pairs, (col, w) + pos per entry
+    if kind == "csr-bb":
+        return base + 4 * delta + 16 * m + 8 * int(deg_in.sum())
+    if kind == "hash":
+        return base + 4 * delta + 16 * m + 8 * int(cap_in.sum())
+    if kind in ("csr-bitset", "csr-bitset-bb"):
+        return base + 4 * delta + 8 * m * wpr
+    if kind == "wswap":
+        return base + 4 * m * ldc
+    raise ValueError(kind)
+
+
+def traffic_from_profiles(kind: str):
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        v = d.get("config2", {}).get(kind)
+        return None if v is None else float(v)
+    except Exception:
+        return None
+
+
+def cpu_baseline_sample(wl, problem, m, budget_s: float = 12.0):
+    """The oracle (exact restatement of the reference loop) on the host cores,
+    over a bounded row sample of one iteration's pair sweep."""
+    from oracle import oracle as O
+    n = wl["n"]
+    op = O.MDP if problem == 0 else O.MAXBS
+    g = O.Graph(n, wl["u"], wl["v"], wl["w"], drop_self_loops=problem == 0)
+    threads = O.max_threads()
+    rows = min(m, max(threads, 64))
+    t, pairs, _, _ = O.sweep_sample(g, op, m=m, rows=rows, seed=1, threads=threads)
+    # grow the sample to the time budget
+    if t > 0:
+        rows = int(min(m, max(rows, rows * budget_s / t / 2)))
+        t, pairs, _, _ = O.sweep_sample(g, op, m=m, rows=rows, sweeps=2, seed=1, threads=threads)
+    return {"value": pairs / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle OpenMP sweep of the start state: {rows} of {m} rows x {n - m} columns, "
+                      f"2 sweeps ({pairs:.3g} pairs, {t:.1f} s)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference loop restated on the host cores (the
+    reference has no CPU implementation and its CUDA build cannot index this
+    instance's 2.5e9 pairs in int32)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    wl = build_workload()
+    n = wl["n"]
+    m = n // 2
+    g = O.Graph(n, wl["u"], wl["v"], wl["w"], drop_self_loops=False)
+    threads = O.max_threads()
+    # size one step so that warmup + steps stay within ~2.5 minutes
+    t1, p1, _, _ = O.sweep_sample(g, O.MAXBS, rows=max(threads, 64), seed=1, threads=threads)
+    per_row = t1 / max(threads, 64)
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    rows = int(max(1, min(m, budget / max(per_row, 1e-9))))
+    for _ in range(args.warmup):
+        O.sweep_sample(g, O.MAXBS, rows=rows, seed=1, threads=threads)
+    tot_t, tot_p = 0.0, 0
+    for _ in range(args.steps):
+        t, p, _, _ = O.sweep_sample(g, O.MAXBS, rows=rows, seed=1, threads=threads)
+        tot_t += t
+        tot_p += p
+    value = tot_p / tot_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded conflict-style graph)",
+        "config": {"workload": WORKLOAD, "sample_rows_per_step": rows, "rows": m, "columns": n - m},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"each step: oracle sweep of {rows} of {m} rows x {n - m} columns"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import ts_b200 as T
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    wl = build_workload(args.workload)
+    n, u, v, w = wl["n"], wl["u"], wl["v"], wl["w"]
+    mdp = wl["problem"] == "mdp"
+    problem = T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS
+    m = wl["m"] if mdp else n // 2
+    P = m * (n - m)
+    kinds = args.structures.split(",") if args.structures else list(T.STRUCT_NAMES)
+    seed = 1 + rank  # replicas: one independent seeded start per rank
+
+    graphs, solvers = {}, {}
+    for k in kinds:
+        g = T.Graph(n, u, v, w, k, drop_self_loops=mdp, stream=stream.cuda_stream)
+        s = T.Solver(g, problem, m=m if mdp else 0, max_iter=10**9, tenure_policy=T.TENURE_FIXED,
+                     tenure=wl["tenure"], piter=500, gamma=150, seed=seed)
+        s.init(None)
+        graphs[k], solvers[k] = g, s
+    total = args.warmup + args.steps
+    for k in kinds:
+        adm = solvers[k].prepare(total)
+        assert adm == total, (k, adm)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    # per-structure compulsory bytes, from the state at the start of the timed region
+    gi = graphs[kinds[0]].info()
+    words = (n + 63) // 64
+    wpr = words + (words & 1)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            for k in kinds:
+                flush.zero_()
+                solvers[k].enqueue(1)
+    torch.cuda.synchronize(dev)
+    sol, _, _, _ = solvers[kinds[0]].state()
+    rowptr = np.zeros(n + 1, np.int64)
+    deg = np.bincount(np.concatenate([u, v]), minlength=n).astype(np.int64)
+    inside = sol[:m]
+    deg_in = deg[inside]
+    cap_in = np.array([_hash_cap(int(d)) for d in deg_in], np.int64)
+    ldc = (n - m + 3) // 4 * 4
+    key_bytes = 4 if 4 * gi.max_weighted_degree < (1 << 30) else 8
+    bytes_per_iter = {k: algorithmic_bytes(k, n, m, ldc, key_bytes, deg_in, cap_in, wpr) for k in kinds}
+    del rowptr
+
+    ev = {k: [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)] for k in kinds}
+    clocks = ClockSampler(local)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    wall0 = time.time()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            for k in kinds:
+                flush.zero_()
+                a, b = ev[k][i]
+                a.record(stream)
+                solvers[k].enqueue(1)
+                b.record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.time() - wall0
+    if ws > 1:
+        dist.barrier()
+    clocks.stop()
+    for k in kinds:
+        it = solvers[k].sync()
+        assert it == total, (k, it, total)
+    per = {}
+    tot_ms = 0.0
+    for k in kinds:
+        ts = [a.elapsed_time(b) for a, b in ev[k]]
+        ms = float(sum(ts))
+        tot_ms += ms
+        avg_s = ms / 1e3 / args.steps
+        per[k] = {"iters_per_s": 1.0 / avg_s, "swap_gains_per_s": P / avg_s, "ms_per_iter": ms / args.steps,
+                  "bytes_per_iter": bytes_per_iter[k], "achieved_gbs": bytes_per_iter[k] / avg_s / 1e9}
+    t_local = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    t_max_ms = float(t_local.item())
+    value = ws * P * len(kinds) * args.steps / (t_max_ms / 1e3)
+
+    peak, peak_src = measured_peaks()
+    dom = max(kinds, key=lambda k: per[k]["ms_per_iter"])
+    achieved = per[dom]["achieved_gbs"]
+    traffic = traffic_from_profiles(dom)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": f"iter_kernel[{dom}]",
+                "peak_source": peak_src}
+
+    line = None
+    if rank == 0:
+        e2e = None if args.no_extras else run_e2e(T, torch, wl, kinds, args, seed, problem, m)
+        cpu = None if args.no_extras else cpu_baseline_sample(wl, problem, m)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded conflict-style graph; MWIS-VR instances are not available offline)",
+            "config": {"workload": wl["desc"], "n": n, "m": m, "pairs_per_iter": P, "structures": kinds,
+                       "l2": "256 MiB buffer written between timed iterations (outside the events)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "iters_per_s": len(kinds) * args.steps / (t_max_ms / 1e3),
+            "per_structure": per,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": len(kinds) * args.steps,
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": wall,
+        }
+    for k in kinds:
+        solvers[k].close()
+        graphs[k].close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+def _hash_cap(deg: int) -> int:
+    cap = 1
+    while cap < deg:
+        cap <<= 1
+    if cap and deg / cap > 0.6:
+        cap <<= 1
+    return max(cap, 2)
+
+
+def run_e2e(T, torch, wl, kinds, args, seed, problem, m):
+    """Same solves through the public C-ABI with host buffers: pinned edge
+    lists uploaded and built per structure, seeded start, `steps` iterations,
+    best bisection read back; wall clock."""
+    n = wl["n"]
+    P = m * (n - m)
+    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (wl["u"], wl["v"], wl["w"])]
+    u, v, w = (x.numpy() for x in pin)
+    h2d = 3 * 4 * len(u)
+    t_tot = 0.0
+    for k in kinds:
+        torch.cuda.synchronize()
+        t0 = time.time()
+        g = T.Graph(n, u, v, w, k, drop_self_loops=problem == T.PROBLEM_MDP)
+        s = T.Solver(g, problem, m=m if problem == T.PROBLEM_MDP else 0, max_iter=args.steps,
+                     tenure_policy=T.TENURE_FIXED, tenure=wl["tenure"], piter=500, gamma=150, seed=seed)
+        s.init(None)
+        s.step(args.steps)
+        r = s.result()
+        t_tot += time.time() - t0
+        assert r.iterations == args.steps and r.device_error == 0
+        s.close()
+        g.close()
+    return {"value": P * len(kinds) * args.steps / t_tot, "unit": UNIT,
+            "h2d_bytes_per_step": h2d * len(kinds) / args.steps,
+            "d2h_bytes_per_step": 4 * (m if problem == T.PROBLEM_MDP else n) * len(kinds) / args.steps,
+            "what": "per structure: ts_graph_create from pinned host edges + ts_solver_init + "
+                    "ts_solver_step(steps) + ts_solver_result, wall clock"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
+                    help="config2 is the benchmark; the others serve profiling")
+    ap.add_argument("--structures", default="", help="comma list (default: all six)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the e2e and CPU-baseline legs")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -166,6 +166,28 @@ __global__ void k_hash_insert(int32_t n, int64_t N, const int64_t* __restrict__ 
   }
 }
 
+// rev[k] for entry k = (y -> z): the entry (z -> y) in row z with the same
+// duplicate rank (a self-loop's entries map to themselves).
+__global__ void k_reverse_index(int32_t n, int64_t N, const int64_t* __restrict__ rowptr,
+                                const int2* __restrict__ adj, int64_t* __restrict__ rev) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t y = row_of(rowptr, n, k);
+    const int32_t z = adj[k].x;
+    auto lower = [&](int32_t row, int32_t key) {
+      int64_t lo = rowptr[row], len = rowptr[row + 1] - lo;
+      while (len > 0) {
+        int64_t half = len >> 1;
+        if (adj[lo + half].x < key) { lo += half + 1; len -= half + 1; }
+        else len = half;
+      }
+      return lo;
+    };
+    const int64_t t = k - lower(y, z);
+    rev[k] = lower(z, y) + t;
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- lookups
@@ -338,6 +360,15 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
   if (h_err[0] & E_HASH_FULL) {
     set_error("ts_graph_create: hash table overflow");
     return TS_ERR_DEVICE;
+  }
+  if (G->kind == TS_STRUCT_CSR) {
+    if ((s = G->rev.alloc(sizeof(int64_t) * (size_t)(N > 0 ? N : 1), "alloc reverse index")) != TS_OK) return s;
+    if (N > 0) {
+      k_reverse_index<<<blocks_for(N), kTPB, 0, st>>>(n, N, G->rowptr.as<int64_t>(), G->adj.as<int2>(),
+                                                      G->rev.as<int64_t>());
+      TS_CUDA(cudaGetLastError());
+    }
+    TS_CUDA(cudaStreamSynchronize(st));
   }
   G->max_wdeg = (int64_t)mw;
   return TS_OK;

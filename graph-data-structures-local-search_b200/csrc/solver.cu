@@ -105,6 +105,14 @@ __global__ void k_init_wswap(const DevGraph g, const DevSolver<KeyT> s) {
   }
 }
 
+// cpos[k] = current position of entry k's neighbour (CSR structure).
+template <class KeyT>
+__global__ void k_init_cpos(const DevGraph g, const DevSolver<KeyT> s) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < g.entries;
+       k += (long long)gridDim.x * blockDim.x)
+    s.cpos[k] = s.pos[g.adj[k].x];
+}
+
 // Objective of a set / bisection given per-vertex flags (1 = inside / side 0).
 __global__ void k_objective(const DevGraph g, int32_t problem, const uint8_t* in,
                             unsigned long long* out) {
@@ -126,11 +134,11 @@ template <int PROB, int ST, class KeyT>
 cudaError_t launch_iter(const DevGraph& g, const DevSolver<KeyT>& s, int grid, size_t smem,
                         cudaStream_t st, int count) {
   auto fn = iter_kernel<PROB, ST, KeyT>;
-  static bool attr_done = false;  // per instantiation
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  static size_t attr_bytes = 48 * 1024;  // per instantiation: largest opt-in so far
+  if (smem > attr_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr_done = true;
+    attr_bytes = smem;
   }
   for (int i = 0; i < count; i++) fn<<<grid, kSweepTPB, smem, st>>>(g, s);
   return cudaGetLastError();
@@ -176,7 +184,7 @@ struct ts_solver {
   int32_t num_pert = 1;
   int64_t log_cap = 0, trace_cap = 0;
   int64_t window_events = 0;
-  DevBuf sol_in, sol_out, vg_in, vg_out, tab_in, tab_out, pos, W, st, recs, movelog, trace, draws;
+  DevBuf sol_in, sol_out, vg_in, vg_out, tab_in, tab_out, pos, W, cpos, st, recs, movelog, trace, draws;
   std::mt19937 rng;
   std::vector<long long> host_draws;  // every perturbation event drawn so far, k draws each
   int64_t events_drawn = 0;
@@ -206,6 +214,7 @@ struct ts_solver {
     s.tab_in = tab_in.as<int32_t>(); s.tab_out = tab_out.as<int32_t>();
     s.pos = pos.as<int32_t>();
     s.W = W.as<int32_t>();
+    s.cpos = cpos.as<int32_t>();
     s.st = st.as<DevState>();
     s.recs = recs.as<CtaRec>();
     s.movelog = movelog.as<int2>();
@@ -329,6 +338,10 @@ ts_status init_device(ts_solver* s, const std::vector<uint8_t>& inside) {
     k_init_wswap<KeyT><<<grid_for((int64_t)m * 32), kInitTPB, 0, st>>>(g, d);
     TS_CUDA(cudaGetLastError());
   }
+  if (s->g->kind == S_CSR && s->g->entries > 0) {
+    k_init_cpos<KeyT><<<grid_for(s->g->entries), kInitTPB, 0, st>>>(g, d);
+    TS_CUDA(cudaGetLastError());
+  }
   unsigned long long obj = 0;
   TS_CUDA(cudaMemcpyAsync(&obj, acc.p, sizeof(obj), cudaMemcpyDeviceToHost, st));
   TS_CUDA(cudaStreamSynchronize(st));
@@ -440,26 +453,36 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   s->wide = 4 * g->max_wdeg >= (1LL << 30);
   s->R = rows_per_tile(g->kind);
   s->n_row_blocks = (m + s->R - 1) / s->R;
-  int64_t want_chunks = (4 * 148 + s->n_row_blocks - 1) / s->n_row_blocks;
+  // Tile geometry.  Staged structures (BB/Hash/Bitset) and MaxBS CSR span the
+  // whole row width once there are enough row blocks, so each CTA stages or
+  // joins its rows once per iteration; MDP CSR keeps a per-column mask in
+  // shared memory (<= 16384 columns); WSwap has no per-CTA setup.
+  const bool mdp_csr = g->kind == S_CSR && p->problem == TS_PROBLEM_MDP;
+  const int64_t full = ((s->delta + kPassCols - 1) / kPassCols) * kPassCols;
+  int64_t max_cols = full;
+  if (g->kind == S_WSWAP) max_cols = 8 * kPassCols;
+  if (mdp_csr) max_cols = 16 * kPassCols;
+  const int64_t min_grid = g->kind == S_WSWAP ? 4 * 148 : 2 * 148;
+  const int64_t want_chunks = std::max<int64_t>(1, (min_grid + s->n_row_blocks - 1) / s->n_row_blocks);
   int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
   cols = ((cols + kPassCols - 1) / kPassCols) * kPassCols;
-  if (cols < kPassCols) cols = kPassCols;
-  if (cols > 8 * kPassCols) cols = 8 * kPassCols;
+  cols = std::max<int64_t>(kPassCols, std::min<int64_t>(cols, max_cols));
   s->chunk_cols = (int32_t)cols;
   s->n_chunks = (int32_t)((s->delta + cols - 1) / cols);
   s->grid = s->n_row_blocks * s->n_chunks;
   if (g->kind == S_CSR) {
     s->stage_bytes = 0;
-    s->dyn_smem = sizeof(uint32_t) * (size_t)s->chunk_cols;
+    s->dyn_smem = mdp_csr ? sizeof(uint32_t) * (size_t)s->chunk_cols : 16;
   } else if (g->kind == S_WSWAP) {
     s->stage_bytes = 0;
     s->dyn_smem = 16;
   } else if (g->kind == S_BITSET || g->kind == S_BITSET_BB) {
-    int64_t b = (int64_t)s->R * g->wpr * 8;
-    s->stage_bytes = (int32_t)std::min<int64_t>(b, 192 * 1024);
+    // bitmap rows first, then room for the rows' CSR segments (hit path)
+    const int64_t b = (int64_t)s->R * g->wpr * 8 + 16 * 1024;
+    s->stage_bytes = (int32_t)std::min<int64_t>(b, 216 * 1024);
     s->dyn_smem = s->stage_bytes;
   } else {
-    s->stage_bytes = 64 * 1024;
+    s->stage_bytes = 96 * 1024;
     s->dyn_smem = s->stage_bytes;
   }
   const int32_t g_eff = std::min(p->gamma, n);
@@ -490,6 +513,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
     size_t rows = (size_t)s->n_row_blocks * s->R;
     A(s->W, sizeof(int32_t) * rows * (size_t)s->ldc, "alloc WSwap matrix");
   }
+  if (g->kind == S_CSR) A(s->cpos, sizeof(int32_t) * (size_t)std::max<int64_t>(1, g->entries), "alloc cpos");
   if (rc == TS_OK) {
     cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&s->h_st), sizeof(DevState));
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMallocHost state");

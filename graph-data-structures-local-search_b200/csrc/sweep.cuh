@@ -11,15 +11,13 @@
 // Each CTA owns a tile of R inside positions (rows) x chunk_cols outside
 // positions (columns) of the m x (n-m) pair space.  It evaluates every pair's
 // gain in 32-bit (or 64-bit) integers, applies the tabu/aspiration filter and
-// keeps a per-row maximum; never materialises a gain array.  The CTA then
-// resolves the lowest flat index achieving its maximum (the CUB ArgMax tie rule,
+// keeps a per-row maximum; no gain array exists.  The CTA then resolves the
+// lowest flat index achieving its maximum (the CUB ArgMax tie rule,
 // cub/thread/thread_operators.cuh:103-121) by rescanning one row, and writes one
 // (key, index) record.  The last CTA to finish reduces the records, decides the
-// move and applies it (contributions along the CSR rows of the two moved
-// vertices, WSwap row/column patches, swap, tabu, best bookkeeping, MaxBS
-// perturbation) -- so the iteration needs no host round trip.
+// move and applies it -- so an iteration needs no host round trip.
 //
-// The fast sweep only tracks allowed pairs (non-tabu, or aspirated).  When no
+// The fast pass only tracks allowed pairs (non-tabu, or aspirated).  When no
 // allowed pair exists (or, for MDP, the best allowed gain is not above the
 // -99999 sentinel), the last CTA switches the state to "exact" and the next
 // launch re-evaluates every pair with the reference's full key rule (MDP
@@ -57,6 +55,10 @@ template <int PROB, class KeyT>
 __device__ __forceinline__ KeyT pair_gain(KeyT rowv, KeyT colv, int32_t w) {
   if (PROB == P_MDP) return colv - rowv - (KeyT)w;  // vg[v] - vg[u] - w(u,v)
   return rowv + colv + (KeyT)2 * (KeyT)w;           // vg[u] + vg[v] + 2 w(u,v)
+}
+
+__device__ __forceinline__ bool allowed(bool row_tabu, bool col_tabu, long long x, long long D) {
+  return !(row_tabu || col_tabu) || x > D;  // GPU-MDP-CSR.cu:580, GPU-MAXBS-CSR.cu:349
 }
 
 __device__ __forceinline__ int32_t warp_max(int32_t v) { return __reduce_max_sync(0xffffffffu, v); }
@@ -102,17 +104,17 @@ __device__ __forceinline__ void load4(const long long* p, long long (&o)[4]) {
   o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
 
-// Staged per-row lookup data (BB / Hash / Bitset): generic pointer into shared
-// memory (or global memory for rows that do not fit the staging budget).
+// Per-row lookup data of the staged structures: generic pointers into shared
+// memory (or global memory for rows past the staging budget).
 struct RowDesc {
-  const void* p;
-  int32_t len;   // BB: entries; Hash: capacity mask; Bitset: CSR degree
-  int32_t pad;
-  long long csr; // Bitset: CSR row start (hit path)
+  const void* p;   // BB: CSR row; Hash: table; Bitset: bitmap words
+  const int2* q;   // Bitset: CSR row (hit path)
+  int32_t len;     // BB / Bitset: CSR degree
+  uint32_t mask;   // Hash: capacity - 1
 };
 
 __device__ __forceinline__ int32_t bb_lower(const int2* a, int32_t len, int32_t v) {
-  // Branch-free lower_bound with a trip count uniform across the warp.
+  // Branch-free lower_bound; the trip count depends on len only (uniform per row).
   int32_t lo = 0;
   int32_t step = len > 0 ? (1 << (31 - __clz(len))) : 0;
   for (; step > 0; step >>= 1)
@@ -131,43 +133,37 @@ __device__ __forceinline__ int32_t hash_probe(const int2* t, uint32_t mask, int3
   return 0;
 }
 
-__device__ __forceinline__ int32_t csr_first(const DevGraph& g, long long start, int32_t deg, int32_t v) {
-  for (int32_t k = 0; k < deg; k++) {
-    int2 e = g.adj[start + k];
-    if (e.x == v) return e.y;
-  }
+__device__ __forceinline__ int32_t scan_first(const int2* a, int32_t len, int32_t v) {
+  for (int32_t k = 0; k < len; k++)
+    if (a[k].x == v) return a[k].y;
   return 0;
 }
 
-__device__ __forceinline__ int32_t csr_lower(const DevGraph& g, long long start, int32_t deg, int32_t v) {
-  return bb_lower(g.adj + start, deg, v);
-}
-
 template <int ST>
-__device__ __forceinline__ int32_t staged_lookup(const DevGraph& g, const RowDesc& d, int32_t v) {
+__device__ __forceinline__ int32_t staged_lookup(const RowDesc& d, int32_t v) {
   if (ST == S_BB) return bb_lower(static_cast<const int2*>(d.p), d.len, v);
-  if (ST == S_HASH) return hash_probe(static_cast<const int2*>(d.p), (uint32_t)d.len, v);
+  if (ST == S_HASH) return hash_probe(static_cast<const int2*>(d.p), d.mask, v);
   // Bitset guard, then the CSR row on a hit (GPU-MDP-CSR-Bitset-BuscaBinaria.cu:598-604).
   const uint64_t* words = static_cast<const uint64_t*>(d.p);
   if (!((words[v >> 6] >> (v & 63)) & 1ull)) return 0;
-  return ST == S_BITSET ? csr_first(g, d.csr, d.len, v) : csr_lower(g, d.csr, d.len, v);
+  return ST == S_BITSET ? scan_first(d.q, d.len, v) : bb_lower(d.q, d.len, v);
 }
 
-// Generic global-memory lookup used by the exact pass and the rescan.
+// Generic global-memory lookup used by the exact pass.
 template <int ST, class KeyT>
 __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSolver<KeyT>& s,
                                                  int32_t row, int32_t col, int32_t u, int32_t v) {
   if (ST == S_WSWAP) return s.W[(long long)row * s.ldc + col];
-  long long st = g.rowptr[u];
-  int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
-  if (ST == S_CSR) return csr_first(g, st, deg, v);
-  if (ST == S_BB) return csr_lower(g, st, deg, v);
+  const long long st = g.rowptr[u];
+  const int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
+  if (ST == S_CSR) return scan_first(g.adj + st, deg, v);
+  if (ST == S_BB) return bb_lower(g.adj + st, deg, v);
   if (ST == S_HASH) {
-    long long b = g.hoff[u];
+    const long long b = g.hoff[u];
     return hash_probe(g.htab + b, (uint32_t)(g.hoff[u + 1] - b - 1), v);
   }
   if (!((g.bits[(long long)u * g.wpr + (v >> 6)] >> (v & 63)) & 1ull)) return 0;
-  return ST == S_BITSET ? csr_first(g, st, deg, v) : csr_lower(g, st, deg, v);
+  return ST == S_BITSET ? scan_first(g.adj + st, deg, v) : bb_lower(g.adj + st, deg, v);
 }
 
 template <class KeyT>
@@ -216,6 +212,7 @@ __device__ long long apply_swap(const DevGraph& g, const DevSolver<KeyT>& s, int
       d = (from_u == z_in) ? -(KeyT)2 * (KeyT)w : (KeyT)2 * (KeyT)w;
     }
     atomic_add_key(vg_at(s, p), d);
+    if (ST == S_CSR) s.cpos[g.rev[at]] = from_u ? m + jv : iu;  // new position of u / v
     const bool first = at == rs || g.adj[at - 1].x != z;
     if (PROB == P_MAXBS && from_u && z == v && first) sh.wuv = w;
     if (ST == S_WSWAP && first && z != (from_u ? u : v)) {
@@ -324,19 +321,18 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
   const int32_t iu = (int32_t)(idx / s.delta), jv = (int32_t)(idx % s.delta);
   int32_t t_u, t_v, t2 = 0;
   if (PROB == P_MDP) {
-    int32_t c1 = s.tenure_policy == 0 ? mdp_ref_tenure(iter) : s.tenure;
+    const int32_t c1 = s.tenure_policy == 0 ? mdp_ref_tenure(iter) : s.tenure;
     int32_t c2 = s.c2_fixed;
     if (s.tenure_policy == 0) c2 = s.c2_tab[c1 == 15 ? 0 : c1 == 30 ? 1 : c1 == 60 ? 2 : 3];
     t_u = c1;  // tab[u] = iter + C1 (GPU-MDP-CSR.cu:549)
     t_v = c2;  // tab[v] = iter + C2 (:550)
     t2 = c2;
   } else {
-    int32_t tt = s.tenure_policy == 0 ? maxbs_ref_tenure(iter, s.maxt) : s.tenure;
+    const int32_t tt = s.tenure_policy == 0 ? maxbs_ref_tenure(iter, s.maxt) : s.tenure;
     t_u = tt;
     t_v = tt;
   }
   apply_swap<PROB, ST, KeyT>(g, s, iu, jv, iter, t_u, t_v, true, sh);
-  bool perturb = false;
   if (threadIdx.x == 0) {
     long long cur = st->cur;
     if (PROB == P_MAXBS && key < kMaxbsRecoverBelow) cur += key + kMaxbsInf;  // :456-460
@@ -352,8 +348,7 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
     }
     trace_rec(s, iter, idx, key, 0, t_u, t2);
     st->iter = iter + 1;
-    if (PROB == P_MAXBS && st->isi >= s.piter) perturb = true;
-    sh.action = perturb ? 3 : 1;
+    sh.action = (PROB == P_MAXBS && st->isi >= s.piter) ? 3 : 1;
   }
   __syncthreads();
   if (PROB == P_MAXBS && sh.action == 3) {
@@ -364,7 +359,7 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
       for (int32_t q = 0; q < s.num_pert; q++) {
         const long long mv = s.draws[ev * s.num_pert + q];
         const int32_t pu = (int32_t)(mv / s.delta), pv = (int32_t)(mv % s.delta);
-        long long aux = apply_swap<PROB, ST, KeyT>(g, s, pu, pv, iter + 1, 0, 0, false, sh);
+        const long long aux = apply_swap<PROB, ST, KeyT>(g, s, pu, pv, iter + 1, 0, 0, false, sh);
         if (threadIdx.x == 0) {
           st->cur += aux;
           st->pert_moves += 1;
@@ -393,7 +388,7 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   const long long iter = st->iter;
   const long long D64 = st->best - st->cur;
   const KeyT D = Lim::clampD(D64);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ KeyT s_rv[R];
@@ -401,6 +396,8 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __shared__ int32_t s_rtab[R];
   __shared__ KeyT s_rowbest[R];
   __shared__ RowDesc s_desc[R];
+  __shared__ long long s_rstart[R];
+  __shared__ int32_t s_off[R + 1];
   __shared__ TailShared sh;
   __shared__ int32_t s_last;
   __shared__ long long s_mc;
@@ -420,12 +417,12 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
     s_rtab[tid] = ok ? (s.tab_in[r0 + tid] > iter) : 0;
     s_rowbest[tid] = Lim::none;
   }
+  __syncthreads();
 
   long long my_key = LLONG_MIN, my_idx = LLONG_MAX;
 
   if (mode == 1) {
     // ---------------- exact pass: the reference's full key rule, int64.
-    __syncthreads();
     for (int32_t r = 0; r < nr; r++) {
       const int32_t u = s_ru[r];
       const long long rv = (long long)s_rv[r];
@@ -437,86 +434,124 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         const bool ct = s.tab_out[c] > iter;
         const int32_t w = global_lookup<ST, KeyT>(g, s, r0 + r, c, u, v);
         const long long x = pair_gain<PROB, long long>(rv, cv, w);
-        const bool allowed = !(rt || ct) || x > D64;
         long long key = x;
-        if (!allowed) key = PROB == P_MDP ? kMdpSentinel : maxbs_penalty(x);
+        if (!allowed(rt, ct, x, D64)) key = PROB == P_MDP ? kMdpSentinel : maxbs_penalty(x);
         better_rec(my_key, my_idx, key, base + c);
       }
     }
     block_best(my_key, my_idx, sh.red);
   } else {
     // ---------------- fast pass
-    uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw);
+    uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw);  // CSR + MDP: adjacency per column
     if (ST == S_CSR) {
-      for (int32_t c = tid; c < s.chunk_cols; c += blockDim.x) s_mask[c] = 0u;
-    }
-    __syncthreads();
-    if (ST == S_CSR) {
-      // Join each row's CSR segment with the chunk by position: marks the
-      // adjacent pairs (mask bit r of column c) and evaluates them exactly.
-      const int warp = tid >> 5, lane = tid & 31;
-      for (int32_t r = warp; r < nr; r += blockDim.x >> 5) {
-        const int32_t u = s_ru[r];
-        const long long a0 = g.rowptr[u], a1 = g.rowptr[u + 1];
-        const KeyT rv = s_rv[r];
-        const bool rt = s_rtab[r] != 0;
-        for (long long k = a0 + lane; k < a1; k += 32) {
-          const int2 e = g.adj[k];
-          if (k > a0 && g.adj[k - 1].x == e.x) continue;  // duplicate pair: first entry wins
-          const int32_t p = s.pos[e.x] - s.m;
-          if (p < c0 || p >= c_end) continue;
-          atomicOr(&s_mask[p - c0], 1u << r);
-          const KeyT x = pair_gain<PROB, KeyT>(rv, s.vg_out[p], e.y);
-          const bool ct = s.tab_out[p] > iter;
-          if (!(rt || ct) || x > D) atomicMax(&s_rowbest[r], x);
+      if (PROB == P_MDP)
+        for (int32_t c = tid; c < s.chunk_cols; c += blockDim.x) s_mask[c] = 0u;
+      if (tid < 32) {
+        // row segments and their prefix (one lane per row)
+        long long a0 = 0;
+        int32_t d = 0;
+        if (lane < nr) {
+          a0 = g.rowptr[s_ru[lane]];
+          d = (int32_t)(g.rowptr[s_ru[lane] + 1] - a0);
+          s_rstart[lane] = a0;
         }
+        int32_t incl = d;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (lane < R) s_off[lane + 1] = incl;
+        if (lane == 0) s_off[0] = 0;
       }
     } else if (ST != S_WSWAP) {
-      // Stage the rows' lookup data in shared memory (rows that do not fit
-      // the budget are read from global memory).
       if (tid == 0) {
         long long off = 0;  // bytes used in the staging area, 16 B aligned
         for (int r = 0; r < R; r++) {
           RowDesc d;
-          d.pad = 0;
-          if (r >= nr) { d.p = nullptr; d.len = 0; d.csr = 0; s_desc[r] = d; continue; }
-          const int32_t u = s_ru[r];
-          const long long rs = g.rowptr[u];
-          const int32_t deg = (int32_t)(g.rowptr[u + 1] - rs);
-          long long bytes;
-          const void* src;
-          if (ST == S_BB) {
-            bytes = 8LL * deg; src = g.adj + rs; d.len = deg; d.csr = rs;
-          } else if (ST == S_HASH) {
-            const long long hb = g.hoff[u];
-            const long long cap = g.hoff[u + 1] - hb;
-            bytes = 8LL * cap; src = g.htab + hb; d.len = (int32_t)(cap - 1); d.csr = hb;
-          } else {
-            bytes = 8LL * g.wpr; src = g.bits + (long long)u * g.wpr; d.len = deg; d.csr = rs;
-          }
-          d.p = src;
-          if (off + bytes <= (long long)s.stage_bytes) {
-            d.p = smem_raw + off;
-            off += (bytes + 15) & ~15LL;
+          d.p = nullptr; d.q = nullptr; d.len = 0; d.mask = 0;
+          if (r < nr) {
+            const int32_t u = s_ru[r];
+            const long long rs = g.rowptr[u];
+            const int32_t deg = (int32_t)(g.rowptr[u + 1] - rs);
+            d.len = deg;
+            if (ST == S_BB) {
+              d.p = g.adj + rs;
+              const long long b = 8LL * deg;
+              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += (b + 15) & ~15LL; }
+            } else if (ST == S_HASH) {
+              const long long hb = g.hoff[u];
+              const long long cap = g.hoff[u + 1] - hb;
+              d.mask = (uint32_t)(cap - 1);
+              d.p = g.htab + hb;
+              const long long b = 8LL * cap;
+              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += (b + 15) & ~15LL; }
+            } else {
+              d.p = g.bits + (long long)u * g.wpr;
+              d.q = g.adj + rs;
+              const long long b = 8LL * g.wpr;
+              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += b; }
+            }
           }
           s_desc[r] = d;
         }
+        if (ST == S_BITSET || ST == S_BITSET_BB) {  // then the CSR rows for the hit path
+          for (int r = 0; r < nr; r++) {
+            const long long b = 8LL * s_desc[r].len;
+            if (off + b <= s.stage_bytes) {
+              s_desc[r].q = reinterpret_cast<const int2*>(smem_raw + off);
+              off += (b + 15) & ~15LL;
+            }
+          }
+        }
       }
-      __syncthreads();
+    }
+    __syncthreads();
+    if (ST == S_CSR) {
+      // Join the rows' CSR segments with the chunk by position: cpos[k] is the
+      // current position of entry k's neighbour, so adjacent pairs of the tile
+      // are found with contiguous reads.  They are evaluated exactly here; for
+      // MDP they are also masked out of the sweep (their w-free gain would be
+      // an over-estimate; for MaxBS it is an under-estimate and harmless).
+      const int32_t total = s_off[nr];
+      for (int32_t f = tid; f < total; f += blockDim.x) {
+        int32_t lo = 0, hi = nr - 1;  // row r with s_off[r] <= f < s_off[r+1]
+        while (lo < hi) {
+          const int32_t mid = (lo + hi + 1) >> 1;
+          if (s_off[mid] <= f) lo = mid; else hi = mid - 1;
+        }
+        const int32_t r = lo;
+        const long long k = s_rstart[r] + (f - s_off[r]);
+        const int32_t c = s.cpos[k] - s.m;
+        if (c < c0 || c >= c_end) continue;
+        const int2 e = g.adj[k];
+        if (k > s_rstart[r] && g.adj[k - 1].x == e.x) continue;  // duplicate pair: first entry wins
+        if (PROB == P_MDP) atomicOr(&s_mask[c - c0], 1u << r);
+        const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], s.vg_out[c], e.y);
+        if (allowed(s_rtab[r] != 0, s.tab_out[c] > iter, (long long)x, (long long)D))
+          atomicMax(&s_rowbest[r], x);
+      }
+    } else if (ST != S_WSWAP) {
       for (int r = 0; r < nr; r++) {
         const RowDesc d = s_desc[r];
-        if (!__isShared(d.p)) continue;
         const int32_t u = s_ru[r];
-        const long long* src;
-        long long words;
-        if (ST == S_BB) { src = reinterpret_cast<const long long*>(g.adj + g.rowptr[u]); words = d.len; }
-        else if (ST == S_HASH) { src = reinterpret_cast<const long long*>(g.htab + g.hoff[u]); words = (long long)d.len + 1; }
-        else { src = reinterpret_cast<const long long*>(g.bits + (long long)u * g.wpr); words = g.wpr; }
-        long long* dst = reinterpret_cast<long long*>(const_cast<void*>(d.p));
-        for (long long q = tid; q < words; q += blockDim.x) dst[q] = __ldg(src + q);
+        if (__isShared(d.p)) {
+          long long words;
+          const long long* src;
+          if (ST == S_BB) { src = reinterpret_cast<const long long*>(g.adj + g.rowptr[u]); words = d.len; }
+          else if (ST == S_HASH) { src = reinterpret_cast<const long long*>(g.htab + g.hoff[u]); words = (long long)d.mask + 1; }
+          else { src = reinterpret_cast<const long long*>(g.bits + (long long)u * g.wpr); words = g.wpr; }
+          long long* dst = reinterpret_cast<long long*>(const_cast<void*>(d.p));
+          for (long long q = tid; q < words; q += blockDim.x) dst[q] = __ldg(src + q);
+        }
+        if ((ST == S_BITSET || ST == S_BITSET_BB) && __isShared(d.q)) {
+          const long long* src = reinterpret_cast<const long long*>(g.adj + g.rowptr[u]);
+          long long* dst = reinterpret_cast<long long*>(const_cast<int2*>(d.q));
+          for (long long q = tid; q < d.len; q += blockDim.x) dst[q] = __ldg(src + q);
+        }
       }
-      __syncthreads();
     }
+    __syncthreads();
 
     KeyT best[R];
 #pragma unroll
@@ -528,9 +563,35 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       if (cb >= c_end) break;
       KeyT cv[4];
       int32_t ct4[4];
+      bool valid[4], ct[4];
+      if (ST == S_WSWAP) {
+        // Issue every row's W load of this pass before using any: the matrix
+        // streams from HBM once per iteration.
+        int4 wv[R];
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          wv[r] = __ldcs(reinterpret_cast<const int4*>(s.W + (long long)(r0 + r) * s.ldc + cb));
+        load4(s.vg_out + cb, cv);
+        load4(s.tab_out + cb, ct4);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          valid[q] = cb + q < c_end;
+          ct[q] = ct4[q] > iter;
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const KeyT t = s_rv[r];
+          const int32_t w4[4] = {wv[r].x, wv[r].y, wv[r].z, wv[r].w};
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], w4[q]);
+            if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+          }
+        }
+        continue;
+      }
       load4(s.vg_out + cb, cv);
       load4(s.tab_out + cb, ct4);
-      bool valid[4], ct[4];
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         valid[q] = cb + q < c_end;
@@ -569,19 +630,6 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
             }
           }
         }
-      } else if (ST == S_WSWAP) {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          const KeyT t = s_rv[r];
-          int32_t w4[4];
-          load4(s.W + (long long)(r0 + r) * s.ldc + cb, w4);
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], w4[q]);
-            const bool ok = valid[q] && (!ct[q] || x > D);
-            if (ok) best[r] = x > best[r] ? x : best[r];
-          }
-        }
       } else {
         int32_t vx[4];
         load4(s.sol_out + cb, vx);
@@ -592,10 +640,9 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
           const RowDesc d = s_desc[r];
 #pragma unroll
           for (int q = 0; q < 4; q++) {
-            const int32_t w = staged_lookup<ST>(g, d, vx[q]);
+            const int32_t w = staged_lookup<ST>(d, vx[q]);
             const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], w);
-            const bool ok = valid[q] && (!ct[q] || x > D);
-            if (ok) best[r] = x > best[r] ? x : best[r];
+            if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
           }
         }
       }
@@ -605,14 +652,14 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
 #pragma unroll
     for (int r = 0; r < R; r++) {
       const KeyT v = warp_max(best[r]);
-      if ((tid & 31) == 0 && v != Lim::none) atomicMax(&s_rowbest[r], v);
+      if (lane == 0 && v != Lim::none) atomicMax(&s_rowbest[r], v);
     }
     __syncthreads();
     if (tid == 0) {
       long long mc = LLONG_MIN;
       int32_t rstar = -1;
       for (int r = 0; r < nr; r++) {
-        KeyT v = s_rowbest[r];
+        const KeyT v = s_rowbest[r];
         if (v == Lim::none) continue;
         if (s_rtab[r] && !(v > D)) continue;  // tabu row: only aspirated pairs
         if ((long long)v > mc) { mc = (long long)v; rstar = r; }
@@ -628,29 +675,43 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       const KeyT target = (KeyT)s_mc;
       const KeyT t = s_rv[r];
       const bool rt = s_rtab[r] != 0;
-      const int32_t u = s_ru[r];
       uint32_t cmin = 0xffffffffu;
       for (int32_t c = c0 + tid; c < c_end; c += blockDim.x) {
-        int32_t w;
+        int32_t w = 0;
         if (ST == S_CSR) {
-          w = ((s_mask[c - c0] >> r) & 1u) ? global_lookup<ST, KeyT>(g, s, r0 + r, c, u, s.sol_out[c]) : 0;
+          // adjacent pairs are matched below from the row's entries; for MaxBS
+          // an adjacent pair's w-free gain can never equal the row maximum.
+          if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
         } else if (ST == S_WSWAP) {
           w = s.W[(long long)(r0 + r) * s.ldc + c];
         } else {
-          w = staged_lookup<ST>(g, s_desc[r], s.sol_out[c]);
+          w = staged_lookup<ST>(s_desc[r], s.sol_out[c]);
         }
         const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], w);
-        const bool ct = s.tab_out[c] > iter;
-        if (x == target && (!(rt || ct) || x > D)) { cmin = (uint32_t)c; break; }
+        if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D)) {
+          cmin = (uint32_t)c;
+          break;
+        }
+      }
+      if (ST == S_CSR) {
+        const long long a0 = s_rstart[r], a1 = a0 + (s_off[r + 1] - s_off[r]);
+        for (long long k = a0 + tid; k < a1; k += blockDim.x) {
+          const int32_t c = s.cpos[k] - s.m;
+          if (c < c0 || c >= c_end) continue;
+          const int2 e = g.adj[k];
+          if (k > a0 && g.adj[k - 1].x == e.x) continue;
+          const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], e.y);
+          if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D) &&
+              (uint32_t)c < cmin)
+            cmin = (uint32_t)c;
+        }
       }
       cmin = __reduce_min_sync(0xffffffffu, cmin);
-      if ((tid & 31) == 0 && cmin != 0xffffffffu) atomicMin(&s_cmin, cmin);
+      if (lane == 0 && cmin != 0xffffffffu) atomicMin(&s_cmin, cmin);
       __syncthreads();
-      if (tid == 0) {
-        if (s_cmin != 0xffffffffu) {
-          my_key = s_mc;
-          my_idx = (long long)(r0 + r) * s.delta + s_cmin;
-        }
+      if (tid == 0 && s_cmin != 0xffffffffu) {
+        my_key = s_mc;
+        my_idx = (long long)(r0 + r) * s.delta + s_cmin;
       }
     }
   }

@@ -44,6 +44,7 @@ struct DevGraph {
   int64_t wpr;
   const int64_t* hoff;
   const int2* htab;
+  const int64_t* rev;  // CSR only: index of the mirrored entry (z->y) of every entry (y->z)
 };
 
 struct alignas(16) CtaRec {
@@ -95,6 +96,7 @@ struct DevSolver {
   int32_t* tab_out;
   int32_t* pos;
   int32_t* W;
+  int32_t* cpos;          // CSR only: cpos[k] = pos[adj[k].x], patched on every move
   DevState* st;
   CtaRec* recs;
   int2* movelog;

@@ -166,6 +166,44 @@ def run(graph: Graph, problem: int, *, m: int = 0, max_iter: int, tenure_policy=
                      trace[:min(r.n_trace, trace_cap)].copy(), sol, pos, tab, vg, best_sol)
 
 
+def sweep_sample(graph: Graph, problem: int, *, m: int = 0, rows: int, sweeps: int = 1,
+                 seed: int = 1, threads: int = 0, initial=None):
+    """Times `sweeps` argmax sweeps over the first `rows` inside positions of the
+    start state (a bounded sample of one iteration's pair evaluation).
+    Returns (seconds, pairs, key, idx)."""
+    L = lib()
+    if not hasattr(L, "_sample_bound"):
+        L.or_sweep_sample.restype = ctypes.c_double
+        L.or_sweep_sample.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Params), ctypes.c_void_p,
+                                      ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int64)]
+        L._sample_bound = True
+    p = _Params()
+    p.problem = problem
+    p.m = m if problem == MDP else graph.n // 2
+    p.max_iter = 1
+    p.tenure_policy = TENURE_FIXED
+    p.tenure_fixed = 1
+    p.maxt = 200
+    p.piter = 500
+    p.gamma = 150
+    p.seed = seed & 0xFFFFFFFF
+    p.init_mode = INIT_RANDOM if initial is None else INIT_EXPLICIT
+    p.threads = threads
+    init = None if initial is None else np.ascontiguousarray(initial, dtype=np.int32)
+    pairs, key, idx = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+    t = L.or_sweep_sample(graph._h, ctypes.byref(p), _ptr(init), rows, sweeps, ctypes.byref(pairs),
+                          ctypes.byref(key), ctypes.byref(idx))
+    if t < 0:
+        raise ValueError("oracle: sweep_sample failed")
+    return float(t), int(pairs.value), int(key.value), int(idx.value)
+
+
+def max_threads() -> int:
+    return os.cpu_count() or 1
+
+
 def mdp_random_initial(n: int, m: int, seed: int) -> np.ndarray:
     out = np.zeros(m, np.int32)
     lib().or_mdp_random_initial(n, m, seed & 0xFFFFFFFF, _ptr(out))

@@ -199,8 +199,9 @@ struct State {
 
 // All-pairs evaluation + ArgMax of one iteration (calculateSwapGain :567-584 /
 // calculateMoveGain :337-353 followed by cub::DeviceReduce::ArgMax).
-Best sweep(const State& s, int problem, int64_t iter, int threads) {
-  const int32_t n = s.n, m = s.m, delta = s.delta;
+Best sweep(const State& s, int problem, int64_t iter, int threads, int32_t row_limit = -1) {
+  const int32_t n = s.n, delta = s.delta;
+  const int32_t m = s.m, rows = row_limit < 0 ? s.m : row_limit;
   std::vector<int64_t> pvg(n);
   std::vector<char> ptab(n);
   for (int32_t p = 0; p < n; p++) {
@@ -221,7 +222,7 @@ Best sweep(const State& s, int problem, int64_t iter, int threads) {
 #ifdef _OPENMP
     t = omp_get_thread_num();
 #endif
-    int32_t r0 = (int32_t)((int64_t)m * t / nt), r1 = (int32_t)((int64_t)m * (t + 1) / nt);
+    int32_t r0 = (int32_t)((int64_t)rows * t / nt), r1 = (int32_t)((int64_t)rows * (t + 1) / nt);
     std::vector<int32_t> stamp(n, -1), wmark(n, 0);
     Best b{INT64_MIN, INT64_MAX};
     for (int32_t i = r0; i < r1; i++) {
@@ -314,11 +315,11 @@ int64_t maxbs_cut(const or_graph* g, const std::vector<int32_t>& part) {
 
 }  // namespace
 
-extern "C" int or_run(const or_graph* g, const or_params* p, const int32_t* initial,
-                      or_result* res, or_trace_rec* trace, int64_t trace_cap,
-                      int32_t* out_sol, int32_t* out_pos, int32_t* out_tab, int64_t* out_vg,
-                      int32_t* out_best_sol) {
-  State s;
+static int build_state(const or_graph* g, const or_params* p, const int32_t* initial, State& s,
+                       std::mt19937& rng, std::vector<int32_t>* part_out);
+
+static int build_state(const or_graph* g, const or_params* p, const int32_t* initial, State& s,
+                       std::mt19937& rng, std::vector<int32_t>* part_out) {
   s.g = g;
   s.n = g->n;
   const int problem = p->problem;
@@ -329,7 +330,6 @@ extern "C" int or_run(const or_graph* g, const or_params* p, const int32_t* init
   const int32_t n = s.n, m = s.m;
   s.sol.assign(n, 0); s.pos.assign(n, 0); s.tab.assign(n, 0); s.vg.assign(n, 0);
   std::vector<char> inside(n, 0);
-  std::mt19937 rng;
   rng.seed(p->seed);
   std::vector<int32_t> part(n, 1);
   if (problem == OR_MDP) {
@@ -375,6 +375,45 @@ extern "C" int or_run(const or_graph* g, const or_params* p, const int32_t* init
     }
     s.cur = maxbs_cut(g, part);
   }
+  s.best = s.cur;
+  if (part_out) *part_out = part;
+  return 0;
+}
+
+extern "C" double or_sweep_sample(const or_graph* g, const or_params* p, const int32_t* initial,
+                                  int32_t rows, int32_t sweeps, int64_t* pairs, int64_t* last_key,
+                                  int64_t* last_idx) {
+  State s;
+  std::mt19937 rng;
+  if (build_state(g, p, initial, s, rng, nullptr) != 0) return -1.0;
+  if (rows < 1 || rows > s.m) rows = s.m;
+  Best b{0, 0};
+  double t0 = 0.0;
+#ifdef _OPENMP
+  t0 = omp_get_wtime();
+#endif
+  for (int32_t k = 0; k < sweeps; k++) b = sweep(s, p->problem, 0, p->threads, rows);
+  double t1 = t0;
+#ifdef _OPENMP
+  t1 = omp_get_wtime();
+#endif
+  if (pairs) *pairs = (int64_t)rows * s.delta * sweeps;
+  if (last_key) *last_key = b.key;
+  if (last_idx) *last_idx = b.idx;
+  return t1 - t0;
+}
+
+extern "C" int or_run(const or_graph* g, const or_params* p, const int32_t* initial,
+                      or_result* res, or_trace_rec* trace, int64_t trace_cap,
+                      int32_t* out_sol, int32_t* out_pos, int32_t* out_tab, int64_t* out_vg,
+                      int32_t* out_best_sol) {
+  State s;
+  std::mt19937 rng;
+  std::vector<int32_t> part;
+  int rc0 = build_state(g, p, initial, s, rng, &part);
+  if (rc0 != 0) return rc0;
+  const int problem = p->problem;
+  const int32_t n = s.n, m = s.m;
   s.best = s.cur;
   std::vector<int32_t> best_sol(s.sol.begin(), s.sol.end());
 

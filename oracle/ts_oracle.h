@@ -95,6 +95,15 @@ int or_run(const or_graph* g, const or_params* p, const int32_t* initial,
            int32_t* out_sol, int32_t* out_pos, int32_t* out_tab, int64_t* out_vg,
            int32_t* out_best_sol);
 
+/* Bounded CPU-baseline sample: from the start state of `p` (initial or the
+ * seeded random start), runs `sweeps` argmax sweeps restricted to the first
+ * `rows` inside positions (rows <= m) with `threads` OpenMP threads and
+ * returns the wall seconds spent in the sweeps; *pairs = pairs evaluated.
+ * The per-pair work is the full loop's. */
+double or_sweep_sample(const or_graph* g, const or_params* p, const int32_t* initial,
+                       int32_t rows, int32_t sweeps, int64_t* pairs, int64_t* last_key,
+                       int64_t* last_idx);
+
 /* Reference tenure schedules, exported for known-answer tests. */
 int32_t or_mdp_tenure(int64_t iter);                  /* GPU-MDP-CSR.cu:461-476 */
 int32_t or_mdp_c2(int32_t c1);                        /* round(0.7*C1) :664 */
