@@ -28,7 +28,7 @@ EXPORTS = [
     "ts_lookup", "ts_lookup_host", "ts_params_default", "ts_solver_create", "ts_solver_init",
     "ts_solver_step", "ts_solver_result", "ts_solver_state", "ts_solver_trace",
     "ts_solver_destroy", "ts_random_start", "ts_perturb_draws", "ts_solver_prepare",
-    "ts_solver_enqueue", "ts_solver_sync",
+    "ts_solver_enqueue", "ts_solver_sync", "ts_best_swap_noalloc",
 ]
 
 

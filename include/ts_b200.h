@@ -208,6 +208,32 @@ ts_status ts_random_start(int32_t problem, int32_t n, int32_t m, uint32_t seed, 
 ts_status ts_perturb_draws(int32_t n, uint32_t seed, int32_t gamma, int32_t init_random,
                            int32_t n_events, int64_t* out);
 
+/* ---------------------------------------------------------------- no allocation
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code recorded in a CUDA stream capture (cudaMalloc is not allowed
+ * there), plugins whose host application owns all of HBM through its own pool,
+ * services held to a fixed device-memory budget.  From a tabu state the caller
+ * keeps in its own device buffers, evaluates every swap of one iteration with
+ * the reference's key rule and ArgMax tie rule and writes the decision; it
+ * allocates nothing, using a fixed scratch array compiled into the library
+ * (about 3 MiB, held on every GPU that loads the library until exit).
+ *   d_rowptr int64[n+1], d_col / d_w int32[entries]: CSR rows sorted by
+ *     neighbour id (the first entry of a duplicated pair is the one used);
+ *   d_sol int32[n]: vertex at each position, the inside set at [0, m);
+ *   d_vg int64[n], d_tab int32[n]: contribution and tabu expiry per vertex;
+ *   iter, cur, best: iteration counter and objective bookkeeping;
+ *   d_out int64[2]: {key, flat index i*(n-m)+(j-m)} of the chosen swap.
+ * n above TS_NOALLOC_MAX_N is rejected (TS_ERR_INVALID_ARG).  Work runs on
+ * `stream` without synchronising.  The first call on a device looks the
+ * scratch address up and should come before any stream capture.  All calls
+ * share the scratch, so calls that overlap on the GPU (other streams or host
+ * threads) race on it. */
+#define TS_NOALLOC_MAX_N 262144
+ts_status ts_best_swap_noalloc(int32_t problem, int32_t n, int32_t m, int64_t iter, int64_t cur,
+                               int64_t best, const int64_t* d_rowptr, const int32_t* d_col,
+                               const int32_t* d_w, const int32_t* d_sol, const int64_t* d_vg,
+                               const int32_t* d_tab, int64_t* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
