@@ -9,7 +9,8 @@
 // device from the edge list: one stable radix sort of 64-bit (row, neighbour)
 // keys produces the CSR; bitset rows and per-vertex hash tables are filled from
 // it.  The hash tables are keyed by (row vertex, neighbour) -- the row selects
-// the table, the neighbour id is the key -- so no aliasing at any n.
+// the table, the neighbour id is the key -- so no aliasing at any n; keys and
+// weights are stored as separate arrays so a probe reads 4 bytes.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -118,49 +119,45 @@ __global__ void k_fill_bits(int32_t n, int64_t N, const int64_t* __restrict__ ro
   }
 }
 
-// Per-vertex capacity: the reference's global rule (GPU-MDP-Hash.cu:430-440)
-// applied per row: power of two >= deg, doubled above load 0.6; at least 2.
-__host__ __device__ __forceinline__ int64_t hash_cap(int64_t deg) {
-  int64_t cap = 1;
-  while (cap < deg) cap <<= 1;
-  if ((float)deg / (float)cap > 0.60f) cap <<= 1;
-  if (cap < 2) cap = 2;
-  return cap;
-}
-
 __global__ void k_hash_caps(int32_t n, const int64_t* __restrict__ rowptr, int64_t* __restrict__ caps) {
   for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
-    caps[r] = hash_cap(rowptr[r + 1] - rowptr[r]);
+    caps[r] = hash_capacity(rowptr[r + 1] - rowptr[r]);
   if (blockIdx.x == 0 && threadIdx.x == 0) caps[n] = 0;
 }
 
-__global__ void k_hash_clear(int64_t slots, int2* __restrict__ tab) {
+__global__ void k_hash_clear(int64_t slots, int32_t* __restrict__ keys, int32_t* __restrict__ vals) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < slots;
-       k += (int64_t)gridDim.x * blockDim.x)
-    tab[k] = make_int2(kHashEmpty, 0);
+       k += (int64_t)gridDim.x * blockDim.x) {
+    keys[k] = kHashEmpty;
+    vals[k] = 0;
+  }
 }
 
 // Inserts the first entry of every (row, neighbour) pair with linear probing.
 __global__ void k_hash_insert(int32_t n, int64_t N, const int64_t* __restrict__ rowptr,
                               const int2* __restrict__ adj, const int64_t* __restrict__ hoff,
-                              int2* __restrict__ tab, int32_t* __restrict__ err) {
+                              int32_t* __restrict__ keys, int32_t* __restrict__ vals,
+                              int32_t* __restrict__ err) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N;
        k += (int64_t)gridDim.x * blockDim.x) {
     int32_t r = row_of(rowptr, n, k);
     int2 e = adj[k];
     if (k > rowptr[r] && adj[k - 1].x == e.x) continue;  // duplicate pair: first wins
-    int64_t base = hoff[r];
-    uint32_t mask = (uint32_t)(hoff[r + 1] - base - 1);
-    uint32_t slot = fmix32((uint32_t)e.x) & mask;
+    const int64_t base = hoff[r];
+    const int64_t cap = hoff[r + 1] - base;
+    const uint32_t gmask = (uint32_t)(cap / 4 - 1);
+    uint32_t grp = hash_group(e.x, hash_gshift(cap));
     bool ok = false;
-    for (uint32_t t = 0; t <= mask; t++) {
-      int prev = atomicCAS(&tab[base + slot].x, kHashEmpty, e.x);
-      if (prev == kHashEmpty) {
-        tab[base + slot].y = e.y;
-        ok = true;
-        break;
+    for (uint32_t t = 0; t <= gmask && !ok; t++) {
+      for (int sl = 0; sl < 4; sl++) {
+        const int64_t at = base + 4LL * grp + sl;
+        if (atomicCAS(&keys[at], kHashEmpty, e.x) == kHashEmpty) {
+          vals[at] = e.y;
+          ok = true;
+          break;
+        }
       }
-      slot = (slot + 1) & mask;
+      grp = (grp + 1) & gmask;
     }
     if (!ok) atomicOr(err, E_HASH_FULL);
   }
@@ -216,14 +213,20 @@ __device__ __forceinline__ int32_t csr_bsearch(const DevGraph& g, int32_t u, int
 __device__ __forceinline__ int32_t lookup_any(const DevGraph& g, int32_t u, int32_t v) {
   switch (g.kind) {
     case S_HASH: {
-      int64_t base = g.hoff[u];
-      uint32_t mask = (uint32_t)(g.hoff[u + 1] - base - 1);
-      uint32_t slot = fmix32((uint32_t)v) & mask;
-      for (uint32_t t = 0; t <= mask; t++) {
-        int2 e = g.htab[base + slot];
-        if (e.x == v) return e.y;
-        if (e.x == kHashEmpty) return 0;
-        slot = (slot + 1) & mask;
+      const int64_t base = g.hoff[u];
+      const int64_t cap = g.hoff[u + 1] - base;
+      const uint32_t gmask = (uint32_t)(cap / 4 - 1);
+      uint32_t grp = hash_group(v, hash_gshift(cap));
+      for (uint32_t t = 0; t <= gmask; t++) {
+        const int4 k4 = *reinterpret_cast<const int4*>(g.hkey + base + 4LL * grp);
+        const int32_t ks[4] = {k4.x, k4.y, k4.z, k4.w};
+        bool empty = false;
+        for (int sl = 0; sl < 4; sl++) {
+          if (ks[sl] == v) return g.hval[base + 4LL * grp + sl];
+          empty |= ks[sl] == kHashEmpty;
+        }
+        if (empty) return 0;
+        grp = (grp + 1) & gmask;
       }
       return 0;
     }
@@ -345,13 +348,14 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
                             cudaMemcpyDeviceToHost, st));
     TS_CUDA(cudaStreamSynchronize(st));
     G->hash_slots = slots;
-    if ((s = G->htab.alloc(sizeof(int2) * slots, "alloc hash table")) != TS_OK) return s;
-    k_hash_clear<<<blocks_for(slots), kTPB, 0, st>>>(slots, G->htab.as<int2>());
+    if ((s = G->hkey.alloc(sizeof(int32_t) * slots, "alloc hash keys")) != TS_OK) return s;
+    if ((s = G->hval.alloc(sizeof(int32_t) * slots, "alloc hash weights")) != TS_OK) return s;
+    k_hash_clear<<<blocks_for(slots), kTPB, 0, st>>>(slots, G->hkey.as<int32_t>(), G->hval.as<int32_t>());
     TS_CUDA(cudaGetLastError());
     if (N > 0) {
       k_hash_insert<<<blocks_for(N), kTPB, 0, st>>>(n, N, G->rowptr.as<int64_t>(), G->adj.as<int2>(),
-                                                    G->hoff.as<int64_t>(), G->htab.as<int2>(),
-                                                    err.as<int32_t>());
+                                                    G->hoff.as<int64_t>(), G->hkey.as<int32_t>(),
+                                                    G->hval.as<int32_t>(), err.as<int32_t>());
       TS_CUDA(cudaGetLastError());
     }
     TS_CUDA(cudaMemcpyAsync(h_err, err.p, sizeof(int32_t) * 2, cudaMemcpyDeviceToHost, st));

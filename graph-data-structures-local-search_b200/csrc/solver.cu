@@ -140,7 +140,7 @@ cudaError_t launch_iter(const DevGraph& g, const DevSolver<KeyT>& s, int grid, s
     if (e != cudaSuccess) return e;
     attr_bytes = smem;
   }
-  for (int i = 0; i < count; i++) fn<<<grid, kSweepTPB, smem, st>>>(g, s);
+  for (int i = 0; i < count; i++) fn<<<grid, Tpb<ST>::v, smem, st>>>(g, s);
   return cudaGetLastError();
 }
 
@@ -458,15 +458,16 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   // joins its rows once per iteration; MDP CSR keeps a per-column mask in
   // shared memory (<= 16384 columns); WSwap has no per-CTA setup.
   const bool mdp_csr = g->kind == S_CSR && p->problem == TS_PROBLEM_MDP;
-  const int64_t full = ((s->delta + kPassCols - 1) / kPassCols) * kPassCols;
+  const int64_t pc = pass_cols_of(g->kind);  // columns one pass of the CTA covers
+  const int64_t full = ((s->delta + pc - 1) / pc) * pc;
   int64_t max_cols = full;
-  if (g->kind == S_WSWAP) max_cols = 8 * kPassCols;
-  if (mdp_csr) max_cols = 16 * kPassCols;
+  if (g->kind == S_WSWAP) max_cols = 8 * pc;
+  if (mdp_csr) max_cols = 16 * pc;
   const int64_t min_grid = g->kind == S_WSWAP ? 4 * 148 : 2 * 148;
   const int64_t want_chunks = std::max<int64_t>(1, (min_grid + s->n_row_blocks - 1) / s->n_row_blocks);
   int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
-  cols = ((cols + kPassCols - 1) / kPassCols) * kPassCols;
-  cols = std::max<int64_t>(kPassCols, std::min<int64_t>(cols, max_cols));
+  cols = ((cols + pc - 1) / pc) * pc;
+  cols = std::max<int64_t>(pc, std::min<int64_t>(cols, max_cols));
   s->chunk_cols = (int32_t)cols;
   s->n_chunks = (int32_t)((s->delta + cols - 1) / cols);
   s->grid = s->n_row_blocks * s->n_chunks;
@@ -476,13 +477,25 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   } else if (g->kind == S_WSWAP) {
     s->stage_bytes = 0;
     s->dyn_smem = 16;
-  } else if (g->kind == S_BITSET || g->kind == S_BITSET_BB) {
-    // bitmap rows first, then room for the rows' CSR segments (hit path)
-    const int64_t b = (int64_t)s->R * g->wpr * 8 + 16 * 1024;
-    s->stage_bytes = (int32_t)std::min<int64_t>(b, 216 * 1024);
-    s->dyn_smem = s->stage_bytes;
   } else {
-    s->stage_bytes = 96 * 1024;
+    // Staging budget sized for rows up to the 90th-percentile degree (larger
+    // rows are read from global memory), so small rows do not cost occupancy.
+    std::vector<int64_t> deg(n);
+    for (int32_t r = 0; r < n; r++) deg[r] = g->h_rowptr[r + 1] - g->h_rowptr[r];
+    std::nth_element(deg.begin(), deg.begin() + (int64_t)n * 9 / 10, deg.end());
+    const int64_t d90 = std::max<int64_t>(1, deg[(int64_t)n * 9 / 10]);
+    auto r16 = [](int64_t b) { return (b + 15) & ~15LL; };
+    int64_t slots = d90;  // keys + weights of one row
+    if (g->kind == S_HASH) slots = hash_capacity(d90);
+    int64_t row_bytes = 2 * r16(4 * slots);
+    if (g->kind == S_BB || g->kind == S_BITSET_BB) {  // + bucket directory
+      int64_t nb = 16;
+      while (nb < d90 / 2 && nb < 4096) nb <<= 1;
+      row_bytes += r16(4 * (nb + 1));
+    }
+    if (g->kind == S_BITSET || g->kind == S_BITSET_BB) row_bytes += 8 * g->wpr;  // bitmap row
+    const int64_t cap = (g->kind == S_BITSET || g->kind == S_BITSET_BB) ? 216 * 1024 : 96 * 1024;
+    s->stage_bytes = (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, s->R * row_bytes));
     s->dyn_smem = s->stage_bytes;
   }
   const int32_t g_eff = std::min(p->gamma, n);

@@ -30,9 +30,15 @@
 
 namespace tsb {
 
-constexpr int kSweepTPB = 256;
 constexpr int kColsPerLane = 4;
-constexpr int kPassCols = kSweepTPB * kColsPerLane;  // 1024 columns per pass
+constexpr int kMaxTPB = 512;
+// Threads per CTA: the bitmap structures stage ~n/8 bytes per row, so they run
+// one large CTA per SM and need more warps in it to hide shared-memory latency.
+template <int ST> struct Tpb { static constexpr int v = 256; };
+template <> struct Tpb<S_BITSET> { static constexpr int v = 512; };
+template <> struct Tpb<S_BITSET_BB> { static constexpr int v = 512; };
+__host__ __device__ inline int tpb_of(int st) { return (st == S_BITSET || st == S_BITSET_BB) ? 512 : 256; }
+__host__ __device__ inline int pass_cols_of(int st) { return tpb_of(st) * kColsPerLane; }
 
 template <int ST> struct Rows { static constexpr int R = 16; };
 template <> struct Rows<S_CSR> { static constexpr int R = 32; };
@@ -104,49 +110,101 @@ __device__ __forceinline__ void load4(const long long* p, long long (&o)[4]) {
   o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
 
-// Per-row lookup data of the staged structures: generic pointers into shared
-// memory (or global memory for rows past the staging budget).
+// Per-row lookup data of the staged structures.  Keys and weights are int32
+// arrays read with a stride: 1 when staged in shared memory (split into a key
+// array and a weight array), 2 when left in the global CSR (interleaved
+// (neighbour, weight) pairs) because the row did not fit the staging budget.
 struct RowDesc {
-  const void* p;   // BB: CSR row; Hash: table; Bitset: bitmap words
-  const int2* q;   // Bitset: CSR row (hit path)
-  int32_t len;     // BB / Bitset: CSR degree
-  uint32_t mask;   // Hash: capacity - 1
+  const int32_t* key;  // BB: CSR keys; Hash: table keys; Bitset: CSR keys (hit path)
+  const int32_t* wt;   // matching weights
+  const uint64_t* bits;  // Bitset: bitmap words of the row
+  int32_t len;         // BB / Bitset: CSR degree
+  int32_t stride;      // 1 staged, 2 global CSR
+  uint32_t mask;       // Hash: number of 4-slot buckets - 1
+  uint32_t shift;      // Hash: 32 - log2(buckets)
+  const int32_t* dir;  // BB rows in shared memory: bucket directory (nullptr: none)
+  int32_t bshift;      // BB: vertex id >> bshift = directory bucket
 };
 
-__device__ __forceinline__ int32_t bb_lower(const int2* a, int32_t len, int32_t v) {
-  // Branch-free lower_bound; the trip count depends on len only (uniform per row).
+// Branch-free lower_bound; the trip count depends on len only (uniform per row).
+template <int STRIDE>
+__device__ __forceinline__ int32_t bb_lower(const int32_t* key, const int32_t* wt, int32_t len, int32_t v) {
   int32_t lo = 0;
   int32_t step = len > 0 ? (1 << (31 - __clz(len))) : 0;
   for (; step > 0; step >>= 1)
-    if (lo + step <= len && a[lo + step - 1].x < v) lo += step;
-  return (lo < len && a[lo].x == v) ? a[lo].y : 0;
+    if (lo + step <= len && key[(lo + step - 1) * STRIDE] < v) lo += step;
+  return (lo < len && key[lo * STRIDE] == v) ? wt[lo * STRIDE] : 0;
+}
+// Binary search of a staged row guided by its bucket directory: dir[b] is the
+// lower bound of the first id of bucket b (ids split into power-of-two
+// ranges, about two row entries per bucket), so the search starts on the
+// one or two entries that can hold v.  Same answer as a lower_bound over the
+// whole row: the first entry of v, or 0.
+__device__ __forceinline__ int32_t dir_lower(const RowDesc& d, int32_t v) {
+  const int32_t b = v >> d.bshift;
+  int32_t lo = d.dir[b], hi = d.dir[b + 1];
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (d.key[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < d.len && d.key[lo] == v) ? d.wt[lo] : 0;
 }
 
-__device__ __forceinline__ int32_t hash_probe(const int2* t, uint32_t mask, int32_t v) {
-  uint32_t slot = fmix32((uint32_t)v) & mask;
-  for (uint32_t k = 0; k <= mask; k++) {
-    int2 e = t[slot];
-    if (e.x == v) return e.y;
-    if (e.x == kHashEmpty) return 0;
-    slot = (slot + 1) & mask;
+__device__ __forceinline__ int32_t bb_lower(const RowDesc& d, int32_t v) {
+  if (d.dir) return dir_lower(d, v);
+  return d.stride == 1 ? bb_lower<1>(d.key, d.wt, d.len, v) : bb_lower<2>(d.key, d.wt, d.len, v);
+}
+
+// Bucketed probe: one 16-byte load reads a whole 4-slot bucket.
+__device__ __forceinline__ int32_t hash_probe(const int32_t* key, const int32_t* wt, uint32_t gmask,
+                                              uint32_t gshift, int32_t v) {
+  uint32_t grp = hash_group(v, gshift);
+  for (uint32_t t = 0; t <= gmask; t++) {
+    const int4 k4 = *reinterpret_cast<const int4*>(key + 4u * grp);
+    if (k4.x == v) return wt[4u * grp];
+    if (k4.y == v) return wt[4u * grp + 1u];
+    if (k4.z == v) return wt[4u * grp + 2u];
+    if (k4.w == v) return wt[4u * grp + 3u];
+    if (k4.x == kHashEmpty || k4.y == kHashEmpty || k4.z == kHashEmpty || k4.w == kHashEmpty) return 0;
+    grp = (grp + 1u) & gmask;
   }
   return 0;
 }
 
-__device__ __forceinline__ int32_t scan_first(const int2* a, int32_t len, int32_t v) {
+template <int STRIDE>
+__device__ __forceinline__ int32_t scan_first(const int32_t* key, const int32_t* wt, int32_t len, int32_t v) {
   for (int32_t k = 0; k < len; k++)
-    if (a[k].x == v) return a[k].y;
+    if (key[k * STRIDE] == v) return wt[k * STRIDE];
   return 0;
 }
 
+// Whole-warp linear scan of a CSR row for v (every lane passes the same v):
+// 32 entries per step, the first match found with a ballot.
+__device__ __forceinline__ int32_t warp_scan_first(const RowDesc& d, int32_t v) {
+  const int lane = threadIdx.x & 31;
+  for (int32_t base = 0; base < d.len; base += 32) {
+    const int32_t k = base + lane;
+    const bool hit = k < d.len && d.key[k * d.stride] == v;
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (b) return d.wt[(base + __ffs(b) - 1) * d.stride];
+  }
+  return 0;
+}
+
+__device__ __forceinline__ bool bit_test(const uint64_t* words, int32_t v) {
+  return (words[v >> 6] >> (v & 63)) & 1ull;
+}
+
+// One lane's lookup in a staged row (the rescan path).
 template <int ST>
 __device__ __forceinline__ int32_t staged_lookup(const RowDesc& d, int32_t v) {
-  if (ST == S_BB) return bb_lower(static_cast<const int2*>(d.p), d.len, v);
-  if (ST == S_HASH) return hash_probe(static_cast<const int2*>(d.p), d.mask, v);
+  if (ST == S_BB) return bb_lower(d, v);
+  if (ST == S_HASH) return hash_probe(d.key, d.wt, d.mask, d.shift, v);
   // Bitset guard, then the CSR row on a hit (GPU-MDP-CSR-Bitset-BuscaBinaria.cu:598-604).
-  const uint64_t* words = static_cast<const uint64_t*>(d.p);
-  if (!((words[v >> 6] >> (v & 63)) & 1ull)) return 0;
-  return ST == S_BITSET ? scan_first(d.q, d.len, v) : bb_lower(d.q, d.len, v);
+  if (!bit_test(d.bits, v)) return 0;
+  if (ST == S_BITSET_BB) return bb_lower(d, v);
+  return d.stride == 1 ? scan_first<1>(d.key, d.wt, d.len, v) : scan_first<2>(d.key, d.wt, d.len, v);
 }
 
 // Generic global-memory lookup used by the exact pass.
@@ -156,14 +214,16 @@ __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSol
   if (ST == S_WSWAP) return s.W[(long long)row * s.ldc + col];
   const long long st = g.rowptr[u];
   const int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
-  if (ST == S_CSR) return scan_first(g.adj + st, deg, v);
-  if (ST == S_BB) return bb_lower(g.adj + st, deg, v);
+  const int32_t* ck = reinterpret_cast<const int32_t*>(g.adj + st);
+  if (ST == S_CSR) return scan_first<2>(ck, ck + 1, deg, v);
+  if (ST == S_BB) return bb_lower<2>(ck, ck + 1, deg, v);
   if (ST == S_HASH) {
     const long long b = g.hoff[u];
-    return hash_probe(g.htab + b, (uint32_t)(g.hoff[u + 1] - b - 1), v);
+    const long long cap = g.hoff[u + 1] - b;
+    return hash_probe(g.hkey + b, g.hval + b, (uint32_t)(cap / 4 - 1), hash_gshift(cap), v);
   }
-  if (!((g.bits[(long long)u * g.wpr + (v >> 6)] >> (v & 63)) & 1ull)) return 0;
-  return ST == S_BITSET ? scan_first(g.adj + st, deg, v) : bb_lower(g.adj + st, deg, v);
+  if (!bit_test(g.bits + (long long)u * g.wpr, v)) return 0;
+  return ST == S_BITSET ? scan_first<2>(ck, ck + 1, deg, v) : bb_lower<2>(ck, ck + 1, deg, v);
 }
 
 template <class KeyT>
@@ -178,7 +238,7 @@ __device__ __forceinline__ void atomic_add_key(long long* a, long long d) {
 
 // ------------------------------------------------------------------ tail
 struct TailShared {
-  CtaRec red[kSweepTPB / 32];
+  CtaRec red[kMaxTPB / 32];
   long long key, idx;
   int32_t action;
   int32_t wuv;
@@ -378,9 +438,10 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
 
 // ------------------------------------------------------------------ kernel
 template <int PROB, int ST, class KeyT>
-__global__ void __launch_bounds__(kSweepTPB)
+__global__ void __launch_bounds__(Tpb<ST>::v)
 iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   constexpr int R = Rows<ST>::R;
+  constexpr int TPB = Tpb<ST>::v;
   using Lim = KeyLim<KeyT>;
   DevState* st = s.st;
   if (st->done || st->iter >= st->target) return;
@@ -469,38 +530,65 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         long long off = 0;  // bytes used in the staging area, 16 B aligned
         for (int r = 0; r < R; r++) {
           RowDesc d;
-          d.p = nullptr; d.q = nullptr; d.len = 0; d.mask = 0;
+          d.key = nullptr; d.wt = nullptr; d.bits = nullptr;
+          d.len = 0; d.stride = 2; d.mask = 0; d.shift = 0; d.dir = nullptr; d.bshift = 0;
           if (r < nr) {
             const int32_t u = s_ru[r];
             const long long rs = g.rowptr[u];
-            const int32_t deg = (int32_t)(g.rowptr[u + 1] - rs);
-            d.len = deg;
-            if (ST == S_BB) {
-              d.p = g.adj + rs;
-              const long long b = 8LL * deg;
-              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += (b + 15) & ~15LL; }
-            } else if (ST == S_HASH) {
+            const int32_t* ck = reinterpret_cast<const int32_t*>(g.adj + rs);
+            d.len = (int32_t)(g.rowptr[u + 1] - rs);
+            if (ST == S_HASH) {
               const long long hb = g.hoff[u];
               const long long cap = g.hoff[u + 1] - hb;
-              d.mask = (uint32_t)(cap - 1);
-              d.p = g.htab + hb;
-              const long long b = 8LL * cap;
-              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += (b + 15) & ~15LL; }
+              d.mask = (uint32_t)(cap / 4 - 1);
+              d.shift = hash_gshift(cap);
+              d.key = g.hkey + hb;
+              d.wt = g.hval + hb;
+              d.stride = 1;
+              const long long b = (4LL * cap + 15) & ~15LL;  // per array
+              if (off + 2 * b <= s.stage_bytes) {
+                d.key = reinterpret_cast<const int32_t*>(smem_raw + off);
+                d.wt = reinterpret_cast<const int32_t*>(smem_raw + off + b);
+                off += 2 * b;
+              }
             } else {
-              d.p = g.bits + (long long)u * g.wpr;
-              d.q = g.adj + rs;
-              const long long b = 8LL * g.wpr;
-              if (off + b <= s.stage_bytes) { d.p = smem_raw + off; off += b; }
+              d.key = ck;  // BB rows, and the Bitset hit path
+              d.wt = ck + 1;
+              if (ST == S_BITSET || ST == S_BITSET_BB) {
+                d.bits = g.bits + (long long)u * g.wpr;
+                const long long b = 8LL * g.wpr;
+                if (off + b <= s.stage_bytes) {
+                  d.bits = reinterpret_cast<const uint64_t*>(smem_raw + off);
+                  off += b;
+                }
+              }
             }
           }
           s_desc[r] = d;
         }
-        if (ST == S_BITSET || ST == S_BITSET_BB) {  // then the CSR rows for the hit path
+        if (ST != S_HASH) {  // CSR rows after the bitmaps, split into keys and weights
+          int32_t lg_n = 0;
+          while ((1LL << lg_n) < (long long)g.n) lg_n++;
           for (int r = 0; r < nr; r++) {
-            const long long b = 8LL * s_desc[r].len;
-            if (off + b <= s.stage_bytes) {
-              s_desc[r].q = reinterpret_cast<const int2*>(smem_raw + off);
-              off += (b + 15) & ~15LL;
+            const int32_t len = s_desc[r].len;
+            const long long b = (4LL * len + 15) & ~15LL;
+            // binary-search rows also get a bucket directory (~2 entries per bucket)
+            int32_t lg_nb = 0;
+            if (ST == S_BB || ST == S_BITSET_BB) {
+              lg_nb = 4;
+              while ((1 << lg_nb) < len / 2 && lg_nb < 12) lg_nb++;
+            }
+            const long long bd = (ST == S_BB || ST == S_BITSET_BB) ? ((4LL * ((1 << lg_nb) + 1) + 15) & ~15LL) : 0;
+            if (off + 2 * b + bd <= s.stage_bytes) {
+              s_desc[r].key = reinterpret_cast<const int32_t*>(smem_raw + off);
+              s_desc[r].wt = reinterpret_cast<const int32_t*>(smem_raw + off + b);
+              s_desc[r].stride = 1;
+              if (bd) {
+                s_desc[r].dir = reinterpret_cast<const int32_t*>(smem_raw + off + 2 * b);
+                s_desc[r].bshift = lg_n > lg_nb ? lg_n - lg_nb : 0;
+                s_desc[r].mask = (uint32_t)(1 << lg_nb);  // buckets (directory has one more entry)
+              }
+              off += 2 * b + bd;
             }
           }
         }
@@ -535,32 +623,68 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       for (int r = 0; r < nr; r++) {
         const RowDesc d = s_desc[r];
         const int32_t u = s_ru[r];
-        if (__isShared(d.p)) {
-          long long words;
-          const long long* src;
-          if (ST == S_BB) { src = reinterpret_cast<const long long*>(g.adj + g.rowptr[u]); words = d.len; }
-          else if (ST == S_HASH) { src = reinterpret_cast<const long long*>(g.htab + g.hoff[u]); words = (long long)d.mask + 1; }
-          else { src = reinterpret_cast<const long long*>(g.bits + (long long)u * g.wpr); words = g.wpr; }
-          long long* dst = reinterpret_cast<long long*>(const_cast<void*>(d.p));
-          for (long long q = tid; q < words; q += blockDim.x) dst[q] = __ldg(src + q);
+        if ((ST == S_BITSET || ST == S_BITSET_BB) && __isShared(d.bits)) {
+          // bitmap rows start on 16 B (wpr is even)
+          const uint4* src = reinterpret_cast<const uint4*>(g.bits + (long long)u * g.wpr);
+          uint4* dst = reinterpret_cast<uint4*>(const_cast<uint64_t*>(d.bits));
+          for (long long q = tid; q < g.wpr / 2; q += TPB) dst[q] = __ldg(src + q);
         }
-        if ((ST == S_BITSET || ST == S_BITSET_BB) && __isShared(d.q)) {
-          const long long* src = reinterpret_cast<const long long*>(g.adj + g.rowptr[u]);
-          long long* dst = reinterpret_cast<long long*>(const_cast<int2*>(d.q));
-          for (long long q = tid; q < d.len; q += blockDim.x) dst[q] = __ldg(src + q);
+        if (__isShared(d.key)) {
+          int32_t* dk = const_cast<int32_t*>(d.key);
+          int32_t* dw = const_cast<int32_t*>(d.wt);
+          if (ST == S_HASH) {
+            const long long hb = g.hoff[u];
+            const long long slots = 4LL * ((long long)d.mask + 1);
+            for (long long q = tid; q < slots; q += TPB) {
+              dk[q] = __ldg(g.hkey + hb + q);
+              dw[q] = __ldg(g.hval + hb + q);
+            }
+          } else {
+            const int2* src = g.adj + g.rowptr[u];
+            for (int32_t q = tid; q < d.len; q += TPB) {
+              const int2 e = __ldg(src + q);
+              dk[q] = e.x;
+              dw[q] = e.y;
+            }
+          }
         }
       }
     }
     __syncthreads();
+    if (ST == S_BB || ST == S_BITSET_BB) {
+      // bucket directories of the staged rows: dir[b] = lower_bound(b << bshift)
+      for (int r = 0; r < nr; r++) {
+        const RowDesc d = s_desc[r];
+        if (!d.dir) continue;
+        int32_t* dd = const_cast<int32_t*>(d.dir);
+        for (int32_t b = tid; b <= (int32_t)d.mask; b += TPB) {
+          const long long lim = (long long)b << d.bshift;
+          int32_t lo = 0, len = d.len;
+          while (len > 0) {
+            const int32_t half = len >> 1;
+            if ((long long)d.key[lo + half] < lim) { lo += half + 1; len -= half + 1; }
+            else len = half;
+          }
+          dd[b] = lo;
+        }
+      }
+      __syncthreads();
+    }
 
-    KeyT best[R];
+    KeyT best[R];  // this thread's maximum per row
 #pragma unroll
     for (int r = 0; r < R; r++) best[r] = Lim::none;
 
-    const int passes = s.chunk_cols / kPassCols;
+    const int passes = s.chunk_cols / (TPB * kColsPerLane);
     for (int pass = 0; pass < passes; pass++) {
-      const int32_t cb = c0 + (pass * kSweepTPB + tid) * kColsPerLane;
-      if (cb >= c_end) break;
+      const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
+      const bool lane_on = cb < c_end;
+      if (ST == S_BITSET) {
+        // the hit path cooperates across the warp: leave the loop together
+        if (__all_sync(0xffffffffu, !lane_on)) break;
+      } else if (!lane_on) {
+        break;
+      }
       KeyT cv[4];
       int32_t ct4[4];
       bool valid[4], ct[4];
@@ -590,11 +714,16 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         }
         continue;
       }
-      load4(s.vg_out + cb, cv);
-      load4(s.tab_out + cb, ct4);
+      if (lane_on) {
+        load4(s.vg_out + cb, cv);
+        load4(s.tab_out + cb, ct4);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++) { cv[q] = 0; ct4[q] = 0; }
+      }
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        valid[q] = cb + q < c_end;
+        valid[q] = lane_on && cb + q < c_end;
         ct[q] = ct4[q] > iter;
       }
       if (ST == S_CSR) {
@@ -631,17 +760,43 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
           }
         }
       } else {
-        int32_t vx[4];
-        load4(s.sol_out + cb, vx);
+        int32_t vx[4] = {0, 0, 0, 0};
+        if (lane_on) load4(s.sol_out + cb, vx);
 #pragma unroll
         for (int r = 0; r < R; r++) {
           if (r >= nr) continue;
           const KeyT t = s_rv[r];
           const RowDesc d = s_desc[r];
+          int32_t wq[4];
+          if (ST == S_BITSET) {
+            // Bit test per pair; each hit is resolved by the whole warp
+            // scanning the row 32 entries at a time (first match by ballot).
+            bool hq[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              hq[q] = valid[q] && bit_test(d.bits, vx[q]);
+              wq[q] = 0;
+            }
+            unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
+            while (any) {
+              const int L = __ffs(any) - 1;
+              any &= any - 1;
+#pragma unroll
+              for (int q = 0; q < 4; q++) {
+                const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
+                if (hv >= 0) {
+                  const int32_t ww = warp_scan_first(d, hv);
+                  if (lane == L) wq[q] = ww;
+                }
+              }
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) wq[q] = valid[q] ? staged_lookup<ST>(d, vx[q]) : 0;
+          }
 #pragma unroll
           for (int q = 0; q < 4; q++) {
-            const int32_t w = staged_lookup<ST>(d, vx[q]);
-            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], w);
+            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
             if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
           }
         }
@@ -675,22 +830,37 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       const KeyT target = (KeyT)s_mc;
       const KeyT t = s_rv[r];
       const bool rt = s_rtab[r] != 0;
+      // Only a thread whose own maximum of this row equals the target swept a
+      // matching column, so only such threads (usually one) rescan their own
+      // columns, in the order they swept them.
+      KeyT mine = Lim::none;
+#pragma unroll
+      for (int rr = 0; rr < R; rr++)
+        if (rr == r) mine = best[rr];
       uint32_t cmin = 0xffffffffu;
-      for (int32_t c = c0 + tid; c < c_end; c += blockDim.x) {
-        int32_t w = 0;
-        if (ST == S_CSR) {
-          // adjacent pairs are matched below from the row's entries; for MaxBS
-          // an adjacent pair's w-free gain can never equal the row maximum.
-          if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
-        } else if (ST == S_WSWAP) {
-          w = s.W[(long long)(r0 + r) * s.ldc + c];
-        } else {
-          w = staged_lookup<ST>(s_desc[r], s.sol_out[c]);
-        }
-        const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], w);
-        if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D)) {
-          cmin = (uint32_t)c;
-          break;
+      if (mine == target) {
+        for (int pass = 0; pass < passes && cmin == 0xffffffffu; pass++) {
+          const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
+          if (cb >= c_end) break;
+          for (int q = 0; q < kColsPerLane; q++) {
+            const int32_t c = cb + q;
+            if (c >= c_end) break;
+            int32_t w = 0;
+            if (ST == S_CSR) {
+              // adjacent pairs are matched below from the row's entries; for
+              // MaxBS an adjacent pair's w-free gain never equals the row maximum.
+              if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
+            } else if (ST == S_WSWAP) {
+              w = s.W[(long long)(r0 + r) * s.ldc + c];
+            } else {
+              w = staged_lookup<ST>(s_desc[r], s.sol_out[c]);
+            }
+            const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], w);
+            if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D)) {
+              cmin = (uint32_t)c;
+              break;
+            }
+          }
         }
       }
       if (ST == S_CSR) {

@@ -65,7 +65,7 @@ struct ts_graph {
   int64_t max_wdeg = 0;
   int64_t wpr = 0;
   int64_t hash_slots = 0;
-  tsb::DevBuf rowptr, adj, bits, hoff, htab, rev;
+  tsb::DevBuf rowptr, adj, bits, hoff, hkey, hval, rev;
   // Host copy of the CSR row pointers/degrees (for footprint planning and the
   // solver's staging budgets); small: n+1 int64.
   std::vector<int64_t> h_rowptr;
@@ -79,11 +79,12 @@ struct ts_graph {
     g.bits = bits.as<uint64_t>();
     g.wpr = wpr;
     g.hoff = hoff.as<int64_t>();
-    g.htab = htab.as<int2>();
+    g.hkey = hkey.as<int32_t>();
+    g.hval = hval.as<int32_t>();
     g.rev = rev.as<int64_t>();
     return g;
   }
   int64_t device_bytes() const {
-    return (int64_t)(rowptr.bytes + adj.bytes + bits.bytes + hoff.bytes + htab.bytes + rev.bytes);
+    return (int64_t)(rowptr.bytes + adj.bytes + bits.bytes + hoff.bytes + hkey.bytes + hval.bytes + rev.bytes);
   }
 };

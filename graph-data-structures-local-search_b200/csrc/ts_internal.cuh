@@ -43,8 +43,9 @@ struct DevGraph {
   const uint64_t* bits;
   int64_t wpr;
   const int64_t* hoff;
-  const int2* htab;
-  const int64_t* rev;  // CSR only: index of the mirrored entry (z->y) of every entry (y->z)
+  const int32_t* hkey;  // Hash: per-vertex tables, keys (neighbour id, -1 empty) ...
+  const int32_t* hval;  // ... and weights, same slots
+  const int64_t* rev;   // CSR only: index of the mirrored entry (z->y) of every entry (y->z)
 };
 
 struct alignas(16) CtaRec {
@@ -107,15 +108,26 @@ struct DevSolver {
   long long draw_events;  // events held in the window
 };
 
-// MurmurHash3 32-bit finaliser (public-domain mixing function), the slot
-// function the reference uses for its GPU hash table (GPU-MDP-Hash.cu:151-158).
-__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t k) {
-  k ^= k >> 16;
-  k *= 0x85ebca6bu;
-  k ^= k >> 13;
-  k *= 0xc2b2ae35u;
-  k ^= k >> 16;
-  return k;
+// Hash structure: one open-addressing table per vertex, keyed by the
+// neighbour id.  The reference keeps one global table at load <= 0.6 with a
+// MurmurHash3 finaliser (GPU-MDP-Hash.cu:151-158,430-440); here the per-vertex
+// tables trade HBM for short probes: capacity = power of two >= 4*degree
+// (load <= 0.25, at least 8 slots), split into 4-slot buckets read with one
+// 16-byte load; the home bucket is a Fibonacci multiplicative hash and a full
+// bucket spills to the next one.  A lookup that meets an empty slot in a
+// bucket without the key is a miss (no deletions ever happen).
+__host__ __device__ __forceinline__ int64_t hash_capacity(int64_t deg) {
+  int64_t cap = 8;
+  while (cap < 4 * deg) cap <<= 1;
+  return cap;
+}
+__host__ __device__ __forceinline__ uint32_t hash_gshift(int64_t cap) {  // 32 - log2(cap / 4)
+  uint32_t l = 0;
+  while ((4LL << l) < cap) l++;
+  return 32u - l;
+}
+__host__ __device__ __forceinline__ uint32_t hash_group(int32_t v, uint32_t gshift) {
+  return ((uint32_t)v * 2654435769u) >> gshift;
 }
 
 // IEEE binary32 round-to-nearest-even of an integer, returned as the exact
