@@ -40,6 +40,68 @@ struct GlibcRand {
   }
 };
 
+// One perturbation event: k distinct flat move indices (GPU-MAXBS-CSR.cu:481-492).
+void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out) {
+  std::unordered_set<long long> used;
+  for (int q = 0; q < k; q++) {
+    long long mv;
+    do {
+      if (P - 1 <= INT32_MAX) {
+        std::uniform_int_distribution<int> d(0, (int)(P - 1));
+        mv = d(rng);
+      } else {  // past the reference's int range (it overflows there)
+        std::uniform_int_distribution<long long> d(0, P - 1);
+        mv = d(rng);
+      }
+    } while (used.count(mv));
+    used.insert(mv);
+    out.push_back(mv);
+  }
+}
+
+void mdp_random_set(int32_t n, int32_t m, uint32_t seed, std::vector<int32_t>& ids) {
+  GlibcRand r(seed);
+  std::vector<uint8_t> used(n, 0);
+  ids.clear();
+  while ((int32_t)ids.size() < m) {
+    int32_t idx = r.next() % n;
+    if (!used[idx]) { used[idx] = 1; ids.push_back(idx); }
+  }
+}
+
+void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0) {
+  std::vector<int> vertices(n);
+  for (int32_t i = 0; i < n; i++) vertices[i] = i;
+  std::shuffle(vertices.begin(), vertices.end(), rng);  // randomPartition :187-195
+  side0.assign(n, 0);
+  for (int32_t i = 0; i < n / 2; i++) side0[vertices[i]] = 1;
+}
+
+int32_t staging_bytes(const ts_graph* g, int R) {
+  // Sized for rows up to the 90th-percentile degree (larger rows are read
+  // from global memory), so small rows do not cost occupancy.
+  if (g->deg90 < 0) {
+    const int32_t n = g->n;
+    std::vector<int64_t> deg(n);
+    for (int32_t r = 0; r < n; r++) deg[r] = g->h_rowptr[r + 1] - g->h_rowptr[r];
+    std::nth_element(deg.begin(), deg.begin() + (int64_t)n * 9 / 10, deg.end());
+    g->deg90 = std::max<int64_t>(1, deg[(int64_t)n * 9 / 10]);
+  }
+  const int64_t d90 = g->deg90;
+  auto r16 = [](int64_t b) { return (b + 15) & ~15LL; };
+  int64_t slots = d90;  // keys + weights of one row
+  if (g->kind == S_HASH) slots = hash_capacity(d90);
+  int64_t row_bytes = 2 * r16(4 * slots);
+  if (g->kind == S_BB || g->kind == S_BITSET_BB) {  // + bucket directory
+    int64_t nb = 16;
+    while (nb < d90 / 2 && nb < 4096) nb <<= 1;
+    row_bytes += r16(4 * (nb + 1));
+  }
+  if (g->kind == S_BITSET || g->kind == S_BITSET_BB) row_bytes += 8 * g->wpr;  // bitmap row
+  const int64_t cap = (g->kind == S_BITSET || g->kind == S_BITSET_BB) ? 216 * 1024 : 96 * 1024;
+  return (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, R * row_bytes));
+}
+
 namespace {
 
 constexpr int kInitTPB = 256;
@@ -252,43 +314,6 @@ ts_status launch_batch(ts_solver* s, int count) {
   return TS_OK;
 }
 
-// One perturbation event: k distinct flat move indices (GPU-MAXBS-CSR.cu:481-492).
-void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out) {
-  std::unordered_set<long long> used;
-  for (int q = 0; q < k; q++) {
-    long long mv;
-    do {
-      if (P - 1 <= INT32_MAX) {
-        std::uniform_int_distribution<int> d(0, (int)(P - 1));
-        mv = d(rng);
-      } else {  // past the reference's int range (it overflows there)
-        std::uniform_int_distribution<long long> d(0, P - 1);
-        mv = d(rng);
-      }
-    } while (used.count(mv));
-    used.insert(mv);
-    out.push_back(mv);
-  }
-}
-
-void mdp_random_set(int32_t n, int32_t m, uint32_t seed, std::vector<int32_t>& ids) {
-  GlibcRand r(seed);
-  std::vector<uint8_t> used(n, 0);
-  ids.clear();
-  while ((int32_t)ids.size() < m) {
-    int32_t idx = r.next() % n;
-    if (!used[idx]) { used[idx] = 1; ids.push_back(idx); }
-  }
-}
-
-void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0) {
-  std::vector<int> vertices(n);
-  for (int32_t i = 0; i < n; i++) vertices[i] = i;
-  std::shuffle(vertices.begin(), vertices.end(), rng);  // randomPartition :187-195
-  side0.assign(n, 0);
-  for (int32_t i = 0; i < n / 2; i++) side0[vertices[i]] = 1;
-}
-
 // MaxBS: make sure the device window holds the draws of every perturbation
 // event that can happen before `target` (events are at least piter apart).
 ts_status prepare_draws(ts_solver* s, int64_t iters_ahead) {
@@ -478,24 +503,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
     s->stage_bytes = 0;
     s->dyn_smem = 16;
   } else {
-    // Staging budget sized for rows up to the 90th-percentile degree (larger
-    // rows are read from global memory), so small rows do not cost occupancy.
-    std::vector<int64_t> deg(n);
-    for (int32_t r = 0; r < n; r++) deg[r] = g->h_rowptr[r + 1] - g->h_rowptr[r];
-    std::nth_element(deg.begin(), deg.begin() + (int64_t)n * 9 / 10, deg.end());
-    const int64_t d90 = std::max<int64_t>(1, deg[(int64_t)n * 9 / 10]);
-    auto r16 = [](int64_t b) { return (b + 15) & ~15LL; };
-    int64_t slots = d90;  // keys + weights of one row
-    if (g->kind == S_HASH) slots = hash_capacity(d90);
-    int64_t row_bytes = 2 * r16(4 * slots);
-    if (g->kind == S_BB || g->kind == S_BITSET_BB) {  // + bucket directory
-      int64_t nb = 16;
-      while (nb < d90 / 2 && nb < 4096) nb <<= 1;
-      row_bytes += r16(4 * (nb + 1));
-    }
-    if (g->kind == S_BITSET || g->kind == S_BITSET_BB) row_bytes += 8 * g->wpr;  // bitmap row
-    const int64_t cap = (g->kind == S_BITSET || g->kind == S_BITSET_BB) ? 216 * 1024 : 96 * 1024;
-    s->stage_bytes = (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, s->R * row_bytes));
+    s->stage_bytes = staging_bytes(g, s->R);
     s->dyn_smem = s->stage_bytes;
   }
   const int32_t g_eff = std::min(p->gamma, n);

@@ -99,14 +99,50 @@ __device__ __forceinline__ void block_best(long long& k, long long& i, CtaRec* s
   __syncthreads();
 }
 
+// Solver-state loads.  The plain kernel (one launch per iteration) reads state
+// through the read-only path: it only changes between launches.  The batched
+// kernel's CTAs read state that their cluster leader changed earlier in the
+// same launch, partly with atomics, so they read it from L2 (ld.global.cg).
+template <bool L2, class T>
+__device__ __forceinline__ T ld_st(const T* p) {
+  if constexpr (L2) return __ldcg(p);
+  else return __ldg(p);
+}
+
+// WSwap matrix rows are streamed once per iteration: evict-first in L2 so they
+// do not push the small per-column arrays out.  The batched form also keeps
+// them out of L1 (never allocated there, so never stale).
+template <bool L2>
+__device__ __forceinline__ int4 ld_w4(const int32_t* p) {
+  if constexpr (L2) {
+    int4 r;
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
+        "ld.global.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], pol;\n\t}"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p));
+    return r;
+  } else {
+    return __ldcs(reinterpret_cast<const int4*>(p));
+  }
+}
+template <bool L2>
+__device__ __forceinline__ int32_t ld_w1(const int32_t* p) {
+  if constexpr (L2) return __ldcg(p);
+  else return *p;
+}
+
 // Column loads: 4 contiguous columns per lane (16 B aligned since ldc % 4 == 0).
+template <bool L2>
 __device__ __forceinline__ void load4(const int32_t* p, int32_t (&o)[4]) {
-  int4 t = __ldg(reinterpret_cast<const int4*>(p));
+  const int4 t = ld_st<L2>(reinterpret_cast<const int4*>(p));
   o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
 }
+template <bool L2>
 __device__ __forceinline__ void load4(const long long* p, long long (&o)[4]) {
-  longlong2 a = __ldg(reinterpret_cast<const longlong2*>(p));
-  longlong2 b = __ldg(reinterpret_cast<const longlong2*>(p) + 1);
+  const longlong2 a = ld_st<L2>(reinterpret_cast<const longlong2*>(p));
+  const longlong2 b = ld_st<L2>(reinterpret_cast<const longlong2*>(p) + 1);
   o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
 
@@ -208,10 +244,10 @@ __device__ __forceinline__ int32_t staged_lookup(const RowDesc& d, int32_t v) {
 }
 
 // Generic global-memory lookup used by the exact pass.
-template <int ST, class KeyT>
+template <int ST, class KeyT, bool L2>
 __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSolver<KeyT>& s,
                                                  int32_t row, int32_t col, int32_t u, int32_t v) {
-  if (ST == S_WSWAP) return s.W[(long long)row * s.ldc + col];
+  if (ST == S_WSWAP) return ld_w1<L2>(s.W + (long long)row * s.ldc + col);
   const long long st = g.rowptr[u];
   const int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
   const int32_t* ck = reinterpret_cast<const int32_t*>(g.adj + st);
@@ -252,7 +288,7 @@ __device__ long long apply_swap(const DevGraph& g, const DevSolver<KeyT>& s, int
                                 long long iter, int32_t t_u, int32_t t_v, bool set_tabu,
                                 TailShared& sh) {
   const int32_t m = s.m;
-  const int32_t u = s.sol_in[iu], v = s.sol_out[jv];
+  const int32_t u = __ldcg(s.sol_in + iu), v = __ldcg(s.sol_out + jv);
   const long long su = g.rowptr[u], sv = g.rowptr[v];
   const int32_t nu = (int32_t)(g.rowptr[u + 1] - su), nv = (int32_t)(g.rowptr[v + 1] - sv);
   if (threadIdx.x == 0) sh.wuv = 0;
@@ -337,17 +373,13 @@ __device__ __forceinline__ void trace_rec(const DevSolver<KeyT>& s, long long it
   st->trace_n = tn + 1;
 }
 
-// Decision + move application by the last CTA.
+// Decision on the iteration's reduced (key, index) -- valid in thread 0 -- and
+// application of the move by the whole CTA: switch to the exact pass, MDP
+// break, or move + tabu + bookkeeping (+ MaxBS perturbation).
 template <int PROB, int ST, class KeyT>
-__device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int mode, TailShared& sh) {
+__device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long k,
+                             long long i, TailShared& sh) {
   DevState* st = s.st;
-  long long k = LLONG_MIN, i = LLONG_MAX;
-  const int nrec = gridDim.x;
-  for (int b = threadIdx.x; b < nrec; b += blockDim.x) {
-    const long long rk = __ldcg(&s.recs[b].key), ri = __ldcg(&s.recs[b].idx);
-    better_rec(k, i, rk, ri);
-  }
-  block_best(k, i, sh.red);
   if (threadIdx.x == 0) {
     int action = 0;  // 0: switch to exact, 1: move, 2: MDP break
     if (mode == 0) {
@@ -372,10 +404,7 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
     }
   }
   __syncthreads();
-  if (sh.action != 1) {
-    if (threadIdx.x == 0) st->counter = 0;
-    return;
-  }
+  if (sh.action != 1) return;
   const long long key = sh.key, idx = sh.idx;
   const long long iter = st->iter;
   const int32_t iu = (int32_t)(idx / s.delta), jv = (int32_t)(idx % s.delta);
@@ -433,21 +462,22 @@ __device__ void iteration_tail(const DevGraph& g, const DevSolver<KeyT>& s, int 
       }
     }
   }
-  if (threadIdx.x == 0) st->counter = 0;
+  __syncthreads();
 }
 
-// ------------------------------------------------------------------ kernel
-template <int PROB, int ST, class KeyT>
-__global__ void __launch_bounds__(Tpb<ST>::v)
-iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
+// ------------------------------------------------------------------ tile
+// Best allowed pair of one tile (row block rb, column chunk ch) in the fast
+// pass (mode 0), or best pair under the full reference key rule (mode 1);
+// (out_key, out_idx) valid in thread 0, (LLONG_MIN, LLONG_MAX) if none.
+// Used once per CTA by the plain kernel and in a loop by the batched one
+// (L2: state loads from L2, see ld_st).
+template <int PROB, int ST, class KeyT, bool L2>
+__device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
+                          long long D64, int rb, int ch, long long& out_key, long long& out_idx,
+                          TailShared& sh) {
   constexpr int R = Rows<ST>::R;
   constexpr int TPB = Tpb<ST>::v;
   using Lim = KeyLim<KeyT>;
-  DevState* st = s.st;
-  if (st->done || st->iter >= st->target) return;
-  const int mode = st->mode;
-  const long long iter = st->iter;
-  const long long D64 = st->best - st->cur;
   const KeyT D = Lim::clampD(D64);
   const int tid = threadIdx.x, lane = tid & 31;
 
@@ -459,13 +489,10 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __shared__ RowDesc s_desc[R];
   __shared__ long long s_rstart[R];
   __shared__ int32_t s_off[R + 1];
-  __shared__ TailShared sh;
-  __shared__ int32_t s_last;
   __shared__ long long s_mc;
   __shared__ int32_t s_rstar;
   __shared__ uint32_t s_cmin;
 
-  const int rb = blockIdx.x / s.n_chunks, ch = blockIdx.x % s.n_chunks;
   const int32_t r0 = rb * R;
   const int32_t nr = min(R, s.m - r0);
   const int32_t c0 = ch * s.chunk_cols;
@@ -473,9 +500,9 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
 
   if (tid < R) {
     const bool ok = tid < nr;
-    s_rv[tid] = ok ? s.vg_in[r0 + tid] : (KeyT)0;
-    s_ru[tid] = ok ? s.sol_in[r0 + tid] : 0;
-    s_rtab[tid] = ok ? (s.tab_in[r0 + tid] > iter) : 0;
+    s_rv[tid] = ok ? ld_st<L2>(s.vg_in + r0 + tid) : (KeyT)0;
+    s_ru[tid] = ok ? ld_st<L2>(s.sol_in + r0 + tid) : 0;
+    s_rtab[tid] = ok ? (ld_st<L2>(s.tab_in + r0 + tid) > iter) : 0;
     s_rowbest[tid] = Lim::none;
   }
   __syncthreads();
@@ -490,10 +517,10 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       const bool rt = s_rtab[r] != 0;
       const long long base = (long long)(r0 + r) * s.delta;
       for (int32_t c = c0 + tid; c < c_end; c += blockDim.x) {
-        const int32_t v = s.sol_out[c];
-        const long long cv = (long long)s.vg_out[c];
-        const bool ct = s.tab_out[c] > iter;
-        const int32_t w = global_lookup<ST, KeyT>(g, s, r0 + r, c, u, v);
+        const int32_t v = ld_st<L2>(s.sol_out + c);
+        const long long cv = (long long)ld_st<L2>(s.vg_out + c);
+        const bool ct = ld_st<L2>(s.tab_out + c) > iter;
+        const int32_t w = global_lookup<ST, KeyT, L2>(g, s, r0 + r, c, u, v);
         const long long x = pair_gain<PROB, long long>(rv, cv, w);
         long long key = x;
         if (!allowed(rt, ct, x, D64)) key = PROB == P_MDP ? kMdpSentinel : maxbs_penalty(x);
@@ -610,13 +637,13 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         }
         const int32_t r = lo;
         const long long k = s_rstart[r] + (f - s_off[r]);
-        const int32_t c = s.cpos[k] - s.m;
+        const int32_t c = ld_st<L2>(s.cpos + k) - s.m;
         if (c < c0 || c >= c_end) continue;
         const int2 e = g.adj[k];
         if (k > s_rstart[r] && g.adj[k - 1].x == e.x) continue;  // duplicate pair: first entry wins
         if (PROB == P_MDP) atomicOr(&s_mask[c - c0], 1u << r);
-        const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], s.vg_out[c], e.y);
-        if (allowed(s_rtab[r] != 0, s.tab_out[c] > iter, (long long)x, (long long)D))
+        const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], ld_st<L2>(s.vg_out + c), e.y);
+        if (allowed(s_rtab[r] != 0, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D))
           atomicMax(&s_rowbest[r], x);
       }
     } else if (ST != S_WSWAP) {
@@ -694,9 +721,9 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         int4 wv[R];
 #pragma unroll
         for (int r = 0; r < R; r++)
-          wv[r] = __ldcs(reinterpret_cast<const int4*>(s.W + (long long)(r0 + r) * s.ldc + cb));
-        load4(s.vg_out + cb, cv);
-        load4(s.tab_out + cb, ct4);
+          wv[r] = ld_w4<L2>(s.W + (long long)(r0 + r) * s.ldc + cb);
+        load4<L2>(s.vg_out + cb, cv);
+        load4<L2>(s.tab_out + cb, ct4);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           valid[q] = cb + q < c_end;
@@ -715,8 +742,8 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         continue;
       }
       if (lane_on) {
-        load4(s.vg_out + cb, cv);
-        load4(s.tab_out + cb, ct4);
+        load4<L2>(s.vg_out + cb, cv);
+        load4<L2>(s.tab_out + cb, ct4);
       } else {
 #pragma unroll
         for (int q = 0; q < 4; q++) { cv[q] = 0; ct4[q] = 0; }
@@ -761,7 +788,7 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
         }
       } else {
         int32_t vx[4] = {0, 0, 0, 0};
-        if (lane_on) load4(s.sol_out + cb, vx);
+        if (lane_on) load4<L2>(s.sol_out + cb, vx);
 #pragma unroll
         for (int r = 0; r < R; r++) {
           if (r >= nr) continue;
@@ -851,12 +878,12 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
               // MaxBS an adjacent pair's w-free gain never equals the row maximum.
               if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
             } else if (ST == S_WSWAP) {
-              w = s.W[(long long)(r0 + r) * s.ldc + c];
+              w = ld_w1<L2>(s.W + (long long)(r0 + r) * s.ldc + c);
             } else {
-              w = staged_lookup<ST>(s_desc[r], s.sol_out[c]);
+              w = staged_lookup<ST>(s_desc[r], ld_st<L2>(s.sol_out + c));
             }
-            const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], w);
-            if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D)) {
+            const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<L2>(s.vg_out + c), w);
+            if (x == target && allowed(rt, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D)) {
               cmin = (uint32_t)c;
               break;
             }
@@ -866,12 +893,12 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
       if (ST == S_CSR) {
         const long long a0 = s_rstart[r], a1 = a0 + (s_off[r + 1] - s_off[r]);
         for (long long k = a0 + tid; k < a1; k += blockDim.x) {
-          const int32_t c = s.cpos[k] - s.m;
+          const int32_t c = ld_st<L2>(s.cpos + k) - s.m;
           if (c < c0 || c >= c_end) continue;
           const int2 e = g.adj[k];
           if (k > a0 && g.adj[k - 1].x == e.x) continue;
-          const KeyT x = pair_gain<PROB, KeyT>(t, s.vg_out[c], e.y);
-          if (x == target && allowed(rt, s.tab_out[c] > iter, (long long)x, (long long)D) &&
+          const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<L2>(s.vg_out + c), e.y);
+          if (x == target && allowed(rt, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D) &&
               (uint32_t)c < cmin)
             cmin = (uint32_t)c;
         }
@@ -886,10 +913,31 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
     }
   }
 
-  if (tid == 0) {
+  out_key = my_key;
+  out_idx = my_idx;
+  __syncthreads();  // the tile's shared arrays are reused by the next call
+}
+
+// ------------------------------------------------------------------ kernel
+// Plain form: one launch = one iteration; CTA b evaluates tile b, the last
+// CTA to finish reduces the records and applies the move.
+template <int PROB, int ST, class KeyT>
+__global__ void __launch_bounds__(Tpb<ST>::v)
+iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
+  DevState* st = s.st;
+  if (st->done || st->iter >= st->target) return;
+  const int mode = st->mode;
+  const long long iter = st->iter;
+  const long long D64 = st->best - st->cur;
+  __shared__ TailShared sh;
+  __shared__ int32_t s_last;
+  long long k, i;
+  tile_eval<PROB, ST, KeyT, false>(g, s, mode, iter, D64, blockIdx.x / s.n_chunks,
+                                   blockIdx.x % s.n_chunks, k, i, sh);
+  if (threadIdx.x == 0) {
     CtaRec rec;
-    rec.key = my_key;
-    rec.idx = my_idx;
+    rec.key = k;
+    rec.idx = i;
     s.recs[blockIdx.x] = rec;
     __threadfence();
     const unsigned prev = atomicAdd(&st->counter, 1u);
@@ -898,7 +946,13 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  iteration_tail<PROB, ST, KeyT>(g, s, mode, sh);
+  k = LLONG_MIN;
+  i = LLONG_MAX;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+    better_rec(k, i, __ldcg(&s.recs[b].key), __ldcg(&s.recs[b].idx));
+  block_best(k, i, sh.red);
+  decide_apply<PROB, ST, KeyT>(g, s, mode, k, i, sh);
+  if (threadIdx.x == 0) st->counter = 0;
 }
 
 }  // namespace tsb

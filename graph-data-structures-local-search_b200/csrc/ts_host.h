@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -87,4 +88,19 @@ struct ts_graph {
   int64_t device_bytes() const {
     return (int64_t)(rowptr.bytes + adj.bytes + bits.bytes + hoff.bytes + hkey.bytes + hval.bytes + rev.bytes);
   }
+  mutable int64_t deg90 = -1;  // 90th-percentile degree, computed on first use
 };
+
+namespace tsb {
+
+// Shared by the plain solver and the batched form (solver.cu).
+// Reference-compatible random streams: the MDP start (srand/rand rejection),
+// the MaxBS shuffle partition (side0[v] = 1: part 0) and one perturbation
+// event of k distinct flat move indices.
+void mdp_random_set(int32_t n, int32_t m, uint32_t seed, std::vector<int32_t>& ids);
+void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0);
+void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out);
+// Dynamic shared memory for staging R rows of a lookup structure.
+int32_t staging_bytes(const ts_graph* g, int R);
+
+}  // namespace tsb

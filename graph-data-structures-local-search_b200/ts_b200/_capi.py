@@ -29,6 +29,8 @@ EXPORTS = [
     "ts_solver_step", "ts_solver_result", "ts_solver_state", "ts_solver_trace",
     "ts_solver_destroy", "ts_random_start", "ts_perturb_draws", "ts_solver_prepare",
     "ts_solver_enqueue", "ts_solver_sync", "ts_best_swap_noalloc",
+    "ts_batch_create", "ts_batch_launch", "ts_batch_sync", "ts_batch_results", "ts_batch_info_get",
+    "ts_batch_destroy", "ts_batch_run",
 ]
 
 
@@ -62,6 +64,26 @@ class Result(ctypes.Structure):
         ("best", ctypes.c_int64), ("best_true", ctypes.c_int64), ("perturbations", ctypes.c_int64),
         ("stopped", ctypes.c_int32), ("m", ctypes.c_int32), ("n", ctypes.c_int32),
         ("device_error", ctypes.c_int32),
+    ]
+
+
+class BatchJob(ctypes.Structure):
+    _fields_ = [
+        ("graph", ctypes.c_void_p), ("params", Params), ("initial", ctypes.c_void_p),
+        ("cluster", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
+    ]
+
+
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("max_bytes", ctypes.c_int64), ("max_slots", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("jobs", ctypes.c_int32), ("groups", ctypes.c_int32), ("slots", ctypes.c_int64),
+        ("slot_bytes", ctypes.c_int64), ("input_bytes", ctypes.c_int64),
+        ("best_sol_words", ctypes.c_int64),
     ]
 
 
@@ -129,6 +151,20 @@ def lib():
     L.ts_random_start.argtypes = [I32, I32, I32, ctypes.c_uint32, P]
     L.ts_perturb_draws.restype = st
     L.ts_perturb_draws.argtypes = [I32, ctypes.c_uint32, I32, I32, I32, P]
+    L.ts_batch_create.restype = st
+    L.ts_batch_create.argtypes = [P, I32, ctypes.POINTER(BatchOpts), P, ctypes.POINTER(P)]
+    L.ts_batch_launch.restype = st
+    L.ts_batch_launch.argtypes = [P]
+    L.ts_batch_sync.restype = st
+    L.ts_batch_sync.argtypes = [P]
+    L.ts_batch_results.restype = st
+    L.ts_batch_results.argtypes = [P, P, P]
+    L.ts_batch_info_get.restype = st
+    L.ts_batch_info_get.argtypes = [P, ctypes.POINTER(BatchInfo)]
+    L.ts_batch_destroy.restype = st
+    L.ts_batch_destroy.argtypes = [P]
+    L.ts_batch_run.restype = st
+    L.ts_batch_run.argtypes = [P, I32, ctypes.POINTER(BatchOpts), P, P]
     _lib = L
     return L
 

@@ -245,3 +245,113 @@ def perturbation_based_tabu_search(graph: Graph, part, piter: int, max_iter: int
         return s.result()
     finally:
         s.close()
+
+
+@dataclass
+class BatchJobSpec:
+    """One solve of a batch: graph, problem parameters and start (None: seeded random)."""
+    graph: Graph
+    problem: int
+    m: int = 0
+    max_iter: int = 50000
+    tenure_policy: int = C.TENURE_REF
+    tenure: int = 15
+    maxt: int = 200
+    piter: int = 500
+    gamma: int = 150
+    seed: int = 1
+    initial: np.ndarray | None = None
+    cluster: int = 0  # CTAs per solve: 0 auto, 1, 2, 4 or 8
+
+
+class Batch:
+    """Many independent solves in one persistent launch, captured as a CUDA graph.
+
+    Each solve gives the result ``Solver(...).init(initial); step(max_iter)``
+    gives for the same graph and parameters (ts_batch_create)."""
+
+    def __init__(self, jobs, *, max_bytes: int = 0, max_slots: int = 0, stream=None):
+        jobs = list(jobs)
+        if not jobs:
+            raise ValueError("a batch needs at least one job")
+        arr = (C.BatchJob * len(jobs))()
+        keep = []  # start arrays must live until create returns
+        self.sizes = []
+        for q, j in enumerate(jobs):
+            p = default_params(j.problem)
+            p.m = j.m
+            p.max_iter = j.max_iter
+            p.tenure_policy = j.tenure_policy
+            p.tenure = j.tenure
+            p.maxt = j.maxt
+            p.piter = j.piter
+            p.gamma = j.gamma
+            p.seed = j.seed & 0xFFFFFFFF
+            arr[q].graph = j.graph.handle.value
+            arr[q].params = p
+            init = None if j.initial is None else np.ascontiguousarray(j.initial, dtype=np.int32)
+            keep.append(init)
+            arr[q].initial = None if init is None else init.ctypes.data
+            arr[q].cluster = j.cluster
+            self.sizes.append(j.m if j.problem == C.PROBLEM_MDP else j.graph.n)
+        self.jobs = jobs
+        opts = C.BatchOpts()
+        opts.max_bytes = max_bytes
+        opts.max_slots = max_slots
+        h = ctypes.c_void_p()
+        st = None if stream is None else ctypes.c_void_p(int(stream))
+        C.check(C.lib().ts_batch_create(arr, len(jobs), ctypes.byref(opts), st, ctypes.byref(h)),
+                "ts_batch_create")
+        self._h = h
+        del keep
+
+    def info(self) -> C.BatchInfo:
+        out = C.BatchInfo()
+        C.check(C.lib().ts_batch_info_get(self._h, ctypes.byref(out)), "ts_batch_info_get")
+        return out
+
+    def launch(self) -> None:
+        C.check(C.lib().ts_batch_launch(self._h), "ts_batch_launch")
+
+    def sync(self) -> None:
+        C.check(C.lib().ts_batch_sync(self._h), "ts_batch_sync")
+
+    def results(self, best_solutions: bool = True) -> list[SolveResult]:
+        n = len(self.jobs)
+        res = (C.Result * n)()
+        words = int(sum(self.sizes))
+        best = np.zeros(max(1, words), np.int32) if best_solutions else None
+        C.check(C.lib().ts_batch_results(self._h, res, C.ptr(best)), "ts_batch_results")
+        out, off = [], 0
+        for q in range(n):
+            r = res[q]
+            sol = best[off:off + self.sizes[q]].copy() if best_solutions else None
+            off += self.sizes[q]
+            out.append(SolveResult(r.iterations, r.evaluations, r.cur, r.best, r.best_true,
+                                   r.perturbations, bool(r.stopped), sol, r.device_error))
+        return out
+
+    def run(self) -> list[SolveResult]:
+        self.launch()
+        self.sync()
+        return self.results()
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            C.lib().ts_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_solve(jobs, **kw) -> list[SolveResult]:
+    """Runs every job once in one batch and returns their results in job order."""
+    b = Batch(jobs, **kw)
+    try:
+        return b.run()
+    finally:
+        b.close()

@@ -208,6 +208,60 @@ ts_status ts_random_start(int32_t problem, int32_t n, int32_t m, uint32_t seed, 
 ts_status ts_perturb_draws(int32_t n, uint32_t seed, int32_t gamma, int32_t init_random,
                            int32_t n_events, int64_t* out);
 
+/* ---------------------------------------------------------------- batched form
+ * Many independent solves (instances, restarts) in one persistent launch per
+ * (problem, structure, key width, CTAs per solve) group, recorded once as a
+ * CUDA graph and replayed.  Stands in for the reference's one-at-a-time
+ * restart loops around tabu_search / perturbationBasedTabuSearch (OBMA
+ * src/mdp/GPU-MDP-CSR.cu:754-903,1146-1208; MACUT
+ * src/maxbisection/GPU-MAXBS-CSR.cu:523-577,679-732).  Every solve gives the
+ * same result as ts_solver_create + ts_solver_init(initial) +
+ * ts_solver_step(max_iter) on its graph and parameters. */
+typedef struct ts_batch ts_batch;
+
+typedef struct ts_batch_job {
+  const ts_graph* graph;    /* all graphs of one batch on one device */
+  ts_params params;         /* params.trace is ignored (no trace in batches) */
+  const int32_t* initial;   /* host, as ts_solver_init; NULL: seeded random start */
+  int32_t cluster;          /* CTAs per solve (a thread-block cluster): 0 auto, or 1, 2, 4, 8 */
+  int32_t reserved[3];      /* zero */
+} ts_batch_job;
+
+typedef struct ts_batch_opts {
+  int64_t max_bytes;        /* HBM budget for solver slots; 0: 60% of free memory */
+  int32_t max_slots;        /* cap on concurrent solves per group; 0: as many as are resident */
+  int32_t reserved[5];      /* zero */
+} ts_batch_opts;
+
+typedef struct ts_batch_info {
+  int32_t jobs;
+  int32_t groups;           /* launches in the captured graph */
+  int64_t slots;            /* concurrent solves, all groups */
+  int64_t slot_bytes;       /* HBM held for solver slots */
+  int64_t input_bytes;      /* HBM held for starts, draws, job table, results */
+  int64_t best_sol_words;   /* int32 words of the packed best solutions */
+} ts_batch_info;
+
+/* Prepares a batch: draws the seeded starts and MaxBS perturbation streams on
+ * host threads, copies them and the job table to the device, sizes solver
+ * slots within the budget and captures the launches as a CUDA graph on
+ * `stream` (a cudaStream_t; NULL: a stream of the library's own).  The graphs
+ * must outlive the batch. */
+ts_status ts_batch_create(const ts_batch_job* jobs, int32_t count, const ts_batch_opts* opts,
+                          void* stream, ts_batch** out);
+/* Replays the captured graph on the batch's stream (asynchronous); every
+ * replay recomputes all solves from their starts. */
+ts_status ts_batch_launch(ts_batch* b);
+ts_status ts_batch_sync(ts_batch* b);
+/* out[count] (may be NULL); best_sols (host, may be NULL) receives the best
+ * solutions packed in job order: MDP m ids in position order, MaxBS part[n]. */
+ts_status ts_batch_results(ts_batch* b, ts_result* out, int32_t* best_sols);
+ts_status ts_batch_info_get(const ts_batch* b, ts_batch_info* out);
+ts_status ts_batch_destroy(ts_batch* b);
+/* create + launch + sync + results + destroy. */
+ts_status ts_batch_run(const ts_batch_job* jobs, int32_t count, const ts_batch_opts* opts,
+                       ts_result* out, int32_t* best_sols);
+
 /* ---------------------------------------------------------------- no allocation
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- code recorded in a CUDA stream capture (cudaMalloc is not allowed

@@ -225,3 +225,15 @@ def test_graph_info_and_errors(gpu):
         s.init(np.zeros(10, np.int32))
     s.close()
     g.close()
+
+
+@pytest.mark.parametrize("kind", ["csr", "wswap", "csr-bb", "hash"])
+def test_int64_keys(gpu, kind):
+    # 4 * max weighted degree >= 2^30 selects 64-bit pair keys
+    n = 120
+    u, v, _ = rand_graph(n, 0.1, 44)
+    w = np.random.default_rng(3).integers(1 << 26, 1 << 27, size=len(u)).astype(np.int32)
+    compare_run(T.PROBLEM_MDP, kind, n, u, v, w, m=20, iters=150, tenure_policy=T.TENURE_FIXED,
+                tenure=9, seed=2)
+    compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=150, tenure_policy=T.TENURE_FIXED,
+                tenure=9, piter=20, gamma=10, seed=2)
