@@ -250,6 +250,7 @@ struct ts_solver {
   std::mt19937 rng;
   std::vector<long long> host_draws;  // every perturbation event drawn so far, k draws each
   int64_t events_drawn = 0;
+  bool external_draws = false;  // perturbation events given by the caller (no more are drawn)
   bool initialized = false;
   int64_t admitted_target = 0;
   DevState* h_st = nullptr;  // pinned mirror
@@ -322,6 +323,10 @@ ts_status prepare_draws(ts_solver* s, int64_t iters_ahead) {
   int64_t need = iters_ahead / std::max(1, s->p.piter) + 2;
   if (need > s->window_events) need = s->window_events;
   const int k = s->num_pert;
+  if (s->external_draws) {
+    // caller's stream: a perturbation past its end sets the device error word
+    need = std::max<int64_t>(0, std::min<int64_t>(need, s->events_drawn - consumed));
+  }
   while (s->events_drawn < consumed + need) {
     draw_event(s->rng, s->P, k, s->host_draws);
     s->events_drawn++;
@@ -553,6 +558,7 @@ ts_status ts_solver_init(ts_solver* s, const int32_t* initial) {
   s->rng.seed(s->p.seed);
   s->host_draws.clear();
   s->events_drawn = 0;
+  s->external_draws = false;
   if (s->p.problem == P_MDP) {
     if (!initial) {
       std::vector<int32_t> ids;
@@ -647,6 +653,38 @@ ts_status finish_batch(ts_solver* s) {
 }  // namespace
 
 extern "C" {
+
+ts_status ts_solver_set_perturbations(ts_solver* s, const int64_t* draws, int64_t n_events) {
+  if (!s || n_events < 0 || (n_events > 0 && !draws)) {
+    set_error("ts_solver_set_perturbations: bad argument");
+    return TS_ERR_INVALID_ARG;
+  }
+  if (!s->initialized) {
+    set_error("ts_solver_set_perturbations: call ts_solver_init first");
+    return TS_ERR_STATE;
+  }
+  if (s->p.problem != P_MAXBS) {
+    set_error("ts_solver_set_perturbations: only Max Bisection perturbs");
+    return TS_ERR_INVALID_ARG;
+  }
+  TS_CUDA(cudaSetDevice(s->g->device));
+  ts_status rc = read_state(s);
+  if (rc != TS_OK) return rc;
+  if (s->h_st->iter != 0 || s->h_st->pert_events != 0) {
+    set_error("ts_solver_set_perturbations: the search has already started");
+    return TS_ERR_STATE;
+  }
+  const int64_t words = n_events * s->num_pert;
+  for (int64_t q = 0; q < words; q++)
+    if (draws[q] < 0 || draws[q] >= s->P) {
+      set_error("ts_solver_set_perturbations: move index out of range");
+      return TS_ERR_INVALID_ARG;
+    }
+  s->host_draws.assign(draws, draws + words);
+  s->events_drawn = n_events;
+  s->external_draws = true;
+  return TS_OK;
+}
 
 ts_status ts_solver_step(ts_solver* s, int64_t k, int64_t* done_iters) {
   if (done_iters) *done_iters = 0;

@@ -102,19 +102,21 @@ __device__ __forceinline__ void block_best(long long& k, long long& i, CtaRec* s
 // Solver-state loads.  The plain kernel (one launch per iteration) reads state
 // through the read-only path: it only changes between launches.  The batched
 // kernel's CTAs read state that their cluster leader changed earlier in the
-// same launch, partly with atomics, so they read it from L2 (ld.global.cg).
-template <bool L2, class T>
+// same launch (plain stores and atomics), so they use ordinary coherent loads
+// (L1-cached; PERSIST): the CTA barrier, and the cluster barrier's
+// release/acquire, make the leader's writes visible to them.
+template <bool PERSIST, class T>
 __device__ __forceinline__ T ld_st(const T* p) {
-  if constexpr (L2) return __ldcg(p);
+  if constexpr (PERSIST) return *p;
   else return __ldg(p);
 }
 
 // WSwap matrix rows are streamed once per iteration: evict-first in L2 so they
 // do not push the small per-column arrays out.  The batched form also keeps
 // them out of L1 (never allocated there, so never stale).
-template <bool L2>
+template <bool PERSIST>
 __device__ __forceinline__ int4 ld_w4(const int32_t* p) {
-  if constexpr (L2) {
+  if constexpr (PERSIST) {
     int4 r;
     asm volatile(
         "{\n\t.reg .b64 pol;\n\t"
@@ -127,22 +129,22 @@ __device__ __forceinline__ int4 ld_w4(const int32_t* p) {
     return __ldcs(reinterpret_cast<const int4*>(p));
   }
 }
-template <bool L2>
+template <bool PERSIST>
 __device__ __forceinline__ int32_t ld_w1(const int32_t* p) {
-  if constexpr (L2) return __ldcg(p);
+  if constexpr (PERSIST) return __ldcg(p);
   else return *p;
 }
 
 // Column loads: 4 contiguous columns per lane (16 B aligned since ldc % 4 == 0).
-template <bool L2>
+template <bool PERSIST>
 __device__ __forceinline__ void load4(const int32_t* p, int32_t (&o)[4]) {
-  const int4 t = ld_st<L2>(reinterpret_cast<const int4*>(p));
+  const int4 t = ld_st<PERSIST>(reinterpret_cast<const int4*>(p));
   o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
 }
-template <bool L2>
+template <bool PERSIST>
 __device__ __forceinline__ void load4(const long long* p, long long (&o)[4]) {
-  const longlong2 a = ld_st<L2>(reinterpret_cast<const longlong2*>(p));
-  const longlong2 b = ld_st<L2>(reinterpret_cast<const longlong2*>(p) + 1);
+  const longlong2 a = ld_st<PERSIST>(reinterpret_cast<const longlong2*>(p));
+  const longlong2 b = ld_st<PERSIST>(reinterpret_cast<const longlong2*>(p) + 1);
   o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
 
@@ -244,10 +246,10 @@ __device__ __forceinline__ int32_t staged_lookup(const RowDesc& d, int32_t v) {
 }
 
 // Generic global-memory lookup used by the exact pass.
-template <int ST, class KeyT, bool L2>
+template <int ST, class KeyT, bool PERSIST>
 __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSolver<KeyT>& s,
                                                  int32_t row, int32_t col, int32_t u, int32_t v) {
-  if (ST == S_WSWAP) return ld_w1<L2>(s.W + (long long)row * s.ldc + col);
+  if (ST == S_WSWAP) return ld_w1<PERSIST>(s.W + (long long)row * s.ldc + col);
   const long long st = g.rowptr[u];
   const int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
   const int32_t* ck = reinterpret_cast<const int32_t*>(g.adj + st);
@@ -470,8 +472,8 @@ __device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mo
 // pass (mode 0), or best pair under the full reference key rule (mode 1);
 // (out_key, out_idx) valid in thread 0, (LLONG_MIN, LLONG_MAX) if none.
 // Used once per CTA by the plain kernel and in a loop by the batched one
-// (L2: state loads from L2, see ld_st).
-template <int PROB, int ST, class KeyT, bool L2>
+// (PERSIST: state written earlier in the same launch, see ld_st).
+template <int PROB, int ST, class KeyT, bool PERSIST>
 __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
                           long long D64, int rb, int ch, long long& out_key, long long& out_idx,
                           TailShared& sh) {
@@ -500,9 +502,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
 
   if (tid < R) {
     const bool ok = tid < nr;
-    s_rv[tid] = ok ? ld_st<L2>(s.vg_in + r0 + tid) : (KeyT)0;
-    s_ru[tid] = ok ? ld_st<L2>(s.sol_in + r0 + tid) : 0;
-    s_rtab[tid] = ok ? (ld_st<L2>(s.tab_in + r0 + tid) > iter) : 0;
+    s_rv[tid] = ok ? ld_st<PERSIST>(s.vg_in + r0 + tid) : (KeyT)0;
+    s_ru[tid] = ok ? ld_st<PERSIST>(s.sol_in + r0 + tid) : 0;
+    s_rtab[tid] = ok ? (ld_st<PERSIST>(s.tab_in + r0 + tid) > iter) : 0;
     s_rowbest[tid] = Lim::none;
   }
   __syncthreads();
@@ -517,10 +519,10 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
       const bool rt = s_rtab[r] != 0;
       const long long base = (long long)(r0 + r) * s.delta;
       for (int32_t c = c0 + tid; c < c_end; c += blockDim.x) {
-        const int32_t v = ld_st<L2>(s.sol_out + c);
-        const long long cv = (long long)ld_st<L2>(s.vg_out + c);
-        const bool ct = ld_st<L2>(s.tab_out + c) > iter;
-        const int32_t w = global_lookup<ST, KeyT, L2>(g, s, r0 + r, c, u, v);
+        const int32_t v = ld_st<PERSIST>(s.sol_out + c);
+        const long long cv = (long long)ld_st<PERSIST>(s.vg_out + c);
+        const bool ct = ld_st<PERSIST>(s.tab_out + c) > iter;
+        const int32_t w = global_lookup<ST, KeyT, PERSIST>(g, s, r0 + r, c, u, v);
         const long long x = pair_gain<PROB, long long>(rv, cv, w);
         long long key = x;
         if (!allowed(rt, ct, x, D64)) key = PROB == P_MDP ? kMdpSentinel : maxbs_penalty(x);
@@ -637,13 +639,13 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         }
         const int32_t r = lo;
         const long long k = s_rstart[r] + (f - s_off[r]);
-        const int32_t c = ld_st<L2>(s.cpos + k) - s.m;
+        const int32_t c = ld_st<PERSIST>(s.cpos + k) - s.m;
         if (c < c0 || c >= c_end) continue;
         const int2 e = g.adj[k];
         if (k > s_rstart[r] && g.adj[k - 1].x == e.x) continue;  // duplicate pair: first entry wins
         if (PROB == P_MDP) atomicOr(&s_mask[c - c0], 1u << r);
-        const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], ld_st<L2>(s.vg_out + c), e.y);
-        if (allowed(s_rtab[r] != 0, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D))
+        const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], ld_st<PERSIST>(s.vg_out + c), e.y);
+        if (allowed(s_rtab[r] != 0, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D))
           atomicMax(&s_rowbest[r], x);
       }
     } else if (ST != S_WSWAP) {
@@ -721,9 +723,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         int4 wv[R];
 #pragma unroll
         for (int r = 0; r < R; r++)
-          wv[r] = ld_w4<L2>(s.W + (long long)(r0 + r) * s.ldc + cb);
-        load4<L2>(s.vg_out + cb, cv);
-        load4<L2>(s.tab_out + cb, ct4);
+          wv[r] = ld_w4<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + cb);
+        load4<PERSIST>(s.vg_out + cb, cv);
+        load4<PERSIST>(s.tab_out + cb, ct4);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           valid[q] = cb + q < c_end;
@@ -742,8 +744,8 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         continue;
       }
       if (lane_on) {
-        load4<L2>(s.vg_out + cb, cv);
-        load4<L2>(s.tab_out + cb, ct4);
+        load4<PERSIST>(s.vg_out + cb, cv);
+        load4<PERSIST>(s.tab_out + cb, ct4);
       } else {
 #pragma unroll
         for (int q = 0; q < 4; q++) { cv[q] = 0; ct4[q] = 0; }
@@ -788,7 +790,7 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         }
       } else {
         int32_t vx[4] = {0, 0, 0, 0};
-        if (lane_on) load4<L2>(s.sol_out + cb, vx);
+        if (lane_on) load4<PERSIST>(s.sol_out + cb, vx);
 #pragma unroll
         for (int r = 0; r < R; r++) {
           if (r >= nr) continue;
@@ -878,12 +880,12 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
               // MaxBS an adjacent pair's w-free gain never equals the row maximum.
               if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
             } else if (ST == S_WSWAP) {
-              w = ld_w1<L2>(s.W + (long long)(r0 + r) * s.ldc + c);
+              w = ld_w1<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + c);
             } else {
-              w = staged_lookup<ST>(s_desc[r], ld_st<L2>(s.sol_out + c));
+              w = staged_lookup<ST>(s_desc[r], ld_st<PERSIST>(s.sol_out + c));
             }
-            const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<L2>(s.vg_out + c), w);
-            if (x == target && allowed(rt, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D)) {
+            const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<PERSIST>(s.vg_out + c), w);
+            if (x == target && allowed(rt, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D)) {
               cmin = (uint32_t)c;
               break;
             }
@@ -893,12 +895,12 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
       if (ST == S_CSR) {
         const long long a0 = s_rstart[r], a1 = a0 + (s_off[r + 1] - s_off[r]);
         for (long long k = a0 + tid; k < a1; k += blockDim.x) {
-          const int32_t c = ld_st<L2>(s.cpos + k) - s.m;
+          const int32_t c = ld_st<PERSIST>(s.cpos + k) - s.m;
           if (c < c0 || c >= c_end) continue;
           const int2 e = g.adj[k];
           if (k > a0 && g.adj[k - 1].x == e.x) continue;
-          const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<L2>(s.vg_out + c), e.y);
-          if (x == target && allowed(rt, ld_st<L2>(s.tab_out + c) > iter, (long long)x, (long long)D) &&
+          const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<PERSIST>(s.vg_out + c), e.y);
+          if (x == target && allowed(rt, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D) &&
               (uint32_t)c < cmin)
             cmin = (uint32_t)c;
         }

@@ -30,7 +30,7 @@ EXPORTS = [
     "ts_solver_destroy", "ts_random_start", "ts_perturb_draws", "ts_solver_prepare",
     "ts_solver_enqueue", "ts_solver_sync", "ts_best_swap_noalloc",
     "ts_batch_create", "ts_batch_launch", "ts_batch_sync", "ts_batch_results", "ts_batch_info_get",
-    "ts_batch_destroy", "ts_batch_run",
+    "ts_batch_destroy", "ts_batch_run", "ts_solver_set_perturbations",
 ]
 
 
@@ -131,6 +131,8 @@ def lib():
     L.ts_solver_create.argtypes = [P, ctypes.POINTER(Params), ctypes.POINTER(P)]
     L.ts_solver_init.restype = st
     L.ts_solver_init.argtypes = [P, P]
+    L.ts_solver_set_perturbations.restype = st
+    L.ts_solver_set_perturbations.argtypes = [P, P, I64]
     L.ts_solver_step.restype = st
     L.ts_solver_step.argtypes = [P, I64, ctypes.POINTER(I64)]
     L.ts_solver_result.restype = st

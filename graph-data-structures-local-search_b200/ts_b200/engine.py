@@ -146,6 +146,16 @@ class Solver:
         arr = None if initial is None else np.ascontiguousarray(initial, dtype=np.int32)
         C.check(C.lib().ts_solver_init(self._h, C.ptr(arr)), "ts_solver_init")
 
+    def set_perturbations(self, draws) -> None:
+        """MaxBS: use the caller's perturbation events (rows of k move indices)."""
+        d = np.ascontiguousarray(draws, dtype=np.int64)
+        n_events = d.shape[0] if d.ndim == 2 else (len(d) // max(1, self._k()))
+        C.check(C.lib().ts_solver_set_perturbations(self._h, C.ptr(d.reshape(-1)), n_events),
+                "ts_solver_set_perturbations")
+
+    def _k(self) -> int:
+        return max(1, min(self.params.gamma, self.n) // 2)
+
     def step(self, k: int) -> int:
         done = ctypes.c_int64(0)
         C.check(C.lib().ts_solver_step(self._h, int(k), ctypes.byref(done)), "ts_solver_step")

@@ -167,6 +167,15 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out);
  *   MaxBS: initial = part[n] in {0,1}, exactly floor(n/2) zeros (host); the
  *     perturbation stream is mt19937(seed) from its start. */
 ts_status ts_solver_init(ts_solver* s, const int32_t* initial);
+/* MaxBS: after ts_solver_init and before the first step, replaces the
+ * perturbation stream with the caller's n_events events of
+ * k = max(1, min(gamma, n)/2) flat move indices each (host, copied).  For
+ * drivers that keep one generator across many searches, as MACUT does: its
+ * perturbationBasedTabuSearch draws from the program-wide mt19937
+ * (src/maxbisection/GPU-MAXBS-CSR.cu:481-492, seeded once at :682).  A search
+ * that needs more events than given stops with TS_ERR_DEVICE; the events it
+ * used are ts_result.perturbations / k. */
+ts_status ts_solver_set_perturbations(ts_solver* s, const int64_t* draws, int64_t n_events);
 /* Runs up to k more iterations on the device (no host round trip per
  * iteration).  Stops early at max_iter or at the MDP all-tabu break.
  * Blocks until they are done; *done_iters (may be NULL) = iterations applied
@@ -261,6 +270,72 @@ ts_status ts_batch_destroy(ts_batch* b);
 /* create + launch + sync + results + destroy. */
 ts_status ts_batch_run(const ts_batch_job* jobs, int32_t count, const ts_batch_opts* opts,
                        ts_result* out, int32_t* best_sols);
+
+/* ---------------------------------------------------------------- served form
+ * A request loop with continuous batching.  Requests (a host edge list plus
+ * solve parameters) are admitted while their estimated HBM footprint fits the
+ * budget; the server builds each graph on the device, keeps graph and tabu
+ * state resident, and advances every admitted solve a bounded number of
+ * iterations per round: small solves as clusters of one persistent launch
+ * (the batched form's kernel), large ones with the plain one-launch-per-
+ * iteration kernel on their own stream, all overlapping on the GPU.  Requests
+ * that arrive meanwhile join at the next round.  A solve's result does not
+ * depend on what else runs: it equals ts_solver_* on the same graph and
+ * parameters.  No counterpart in the reference, which runs one search per
+ * process (src/run_experimentos.py:101-117). */
+typedef struct ts_server ts_server;
+
+typedef struct ts_request {
+  int32_t n;
+  int64_t num_edges;
+  const int32_t* u;          /* host, copied by ts_server_submit */
+  const int32_t* v;
+  const int32_t* w;
+  int32_t kind;              /* ts_struct, or -1: the server's choice by size */
+  int32_t drop_self_loops;
+  ts_params params;
+  const int32_t* initial;    /* host, copied; NULL: seeded random start */
+  int32_t* best_sol;         /* host, may be NULL; written before completion is reported;
+                                MDP m ids, MaxBS part[n]; must stay valid until then */
+} ts_request;
+
+typedef struct ts_server_opts {
+  int64_t max_bytes;         /* HBM budget for admitted requests; 0: 60% of free memory */
+  double round_ms;           /* target duration of one round; 0: 5 ms */
+  int64_t plain_min_pairs;   /* pairs per iteration from which a solve runs plain; 0: 2^20 */
+  int32_t reserved[8];
+} ts_server_opts;
+
+typedef struct ts_served {
+  int64_t ticket;
+  int32_t status;            /* ts_status of the request */
+  int32_t executor;          /* 0 packed (cluster of a persistent launch), 1 plain */
+  int32_t kind;              /* structure used */
+  int32_t pad;
+  ts_result result;
+  double submit_s, admit_s, done_s;   /* server clock, seconds */
+  int64_t footprint_bytes;
+} ts_served;
+
+typedef struct ts_server_stats {
+  int64_t submitted, admitted, completed, queued, active;
+  int64_t rounds;
+  int64_t bytes_in_use, bytes_budget;
+  double busy_s;             /* time with at least one admitted request */
+} ts_server_stats;
+
+/* Starts the scheduler thread on the current device. */
+ts_status ts_server_create(const ts_server_opts* opts, ts_server** out);
+/* Queues a request (copies its arrays); *ticket identifies it. */
+ts_status ts_server_submit(ts_server* s, const ts_request* req, int64_t* ticket);
+/* Copies up to cap completed requests to out (oldest first), waiting up to
+ * wait_ms for the first one; *n_out = records copied. */
+ts_status ts_server_poll(ts_server* s, ts_served* out, int32_t cap, int32_t* n_out, int32_t wait_ms);
+ts_status ts_server_stats_get(ts_server* s, ts_server_stats* out);
+/* Seconds on the server clock (the clock of submit_s / admit_s / done_s). */
+double ts_server_now(const ts_server* s);
+/* Stops the scheduler after the admitted and queued requests complete. */
+ts_status ts_server_destroy(ts_server* s);
 
 /* ---------------------------------------------------------------- no allocation
  * No counterpart in the reference.  For callers that cannot allocate device
