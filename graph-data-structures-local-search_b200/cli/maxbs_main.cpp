@@ -7,6 +7,7 @@
 //     -gens G          G generations, no time limit (deterministic runs)
 //     -tenure ref|fixed:T
 //     -alg NAME        lookup structure (default: from the program name)
+//     -check-instance  print the parsed instance (n m edges scale weight-sum) and exit
 #include <ctime>
 #include <fstream>
 #include <iomanip>
@@ -43,6 +44,7 @@ int main(int argc, char** argv) {
   cfg.seed = (unsigned)time(nullptr);
   std::string out_file;
   int32_t kind = struct_from_program(argv[0], "maxbs");
+  bool check_only = false;
   try {
     Instance I = read_maxbs(argv[1]);
     for (int a = 2; a < argc; a++) {
@@ -62,11 +64,18 @@ int main(int argc, char** argv) {
       else if (o == "-gens") cfg.max_generations = std::stoll(next());
       else if (o == "-tenure") parse_tenure(next(), &cfg.tenure_policy, &cfg.tenure);
       else if (o == "-alg") kind = ts_struct_from_name(next().c_str());
+      else if (o == "-check-instance") check_only = true;
       else {
         std::cerr << "Opcao desconhecida: " << o << "\n";
         usage(argv[0]);
         return 1;
       }
+    }
+    if (check_only) {
+      long long sum = 0;
+      for (int32_t x : I.w) sum += x;
+      std::printf("%d %d %zu %lld %lld %d\n", I.n, I.m, I.w.size(), (long long)I.scale, sum, I.rounded ? 1 : 0);
+      return 0;
     }
     if (kind < 0) kind = TS_STRUCT_CSR;
     if (cfg.p < 1 || cfg.piter < 1 || cfg.maxt < 1 || cfg.max_iter < 0 || cfg.gamma < 0)

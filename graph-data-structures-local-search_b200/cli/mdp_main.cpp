@@ -11,6 +11,7 @@
 //     --tenure ref|fixed:T
 //     --alg NAME      lookup structure (default: from the program name)
 //     --quiet         no per-search lines
+//     --check-instance  print the parsed instance (n m edges scale weight-sum) and exit
 #include <cmath>
 #include <ctime>
 #include <iomanip>
@@ -37,6 +38,7 @@ int main(int argc, char** argv) {
   ObmaConfig cfg;
   int32_t kind = struct_from_program(argv[0], "mdp");
   int32_t m_override = 0;
+  bool check_only = false;
   try {
     for (int a = 5; a < argc; a++) {
       const std::string o = argv[a];
@@ -51,6 +53,7 @@ int main(int argc, char** argv) {
       else if (o == "--tenure") parse_tenure(next(), &cfg.tenure_policy, &cfg.tenure);
       else if (o == "--alg") kind = ts_struct_from_name(next().c_str());
       else if (o == "--quiet") cfg.verbose = false;
+      else if (o == "--check-instance") check_only = true;
       else throw std::runtime_error("unknown option " + o);
     }
     if (kind < 0) kind = TS_STRUCT_CSR;
@@ -58,6 +61,12 @@ int main(int argc, char** argv) {
 
     Instance I = read_mdp(instance_name, dataset);
     if (m_override > 0) I.m = m_override;
+    if (check_only) {
+      long long sum = 0;
+      for (int32_t x : I.w) sum += x;
+      std::printf("%d %d %zu %lld %lld %d\n", I.n, I.m, I.w.size(), (long long)I.scale, sum, I.rounded ? 1 : 0);
+      return 0;
+    }
     std::cout << "Dataset: " << dataset << std::endl;
     if (dataset.rfind("MDG", 0) == 0) std::cout << I.n << "-" << I.m << std::endl;
     const double density = (double)I.declared_edges / ((double)I.n * (I.n - 1) / 2.0);

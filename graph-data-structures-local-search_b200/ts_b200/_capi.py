@@ -31,6 +31,8 @@ EXPORTS = [
     "ts_solver_enqueue", "ts_solver_sync", "ts_best_swap_noalloc",
     "ts_batch_create", "ts_batch_launch", "ts_batch_sync", "ts_batch_results", "ts_batch_info_get",
     "ts_batch_destroy", "ts_batch_run", "ts_solver_set_perturbations",
+    "ts_server_create", "ts_server_submit", "ts_server_poll", "ts_server_stats_get", "ts_server_now",
+    "ts_server_destroy",
 ]
 
 
@@ -84,6 +86,37 @@ class BatchInfo(ctypes.Structure):
         ("jobs", ctypes.c_int32), ("groups", ctypes.c_int32), ("slots", ctypes.c_int64),
         ("slot_bytes", ctypes.c_int64), ("input_bytes", ctypes.c_int64),
         ("best_sol_words", ctypes.c_int64),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32), ("num_edges", ctypes.c_int64), ("u", ctypes.c_void_p),
+        ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("kind", ctypes.c_int32),
+        ("drop_self_loops", ctypes.c_int32), ("params", Params), ("initial", ctypes.c_void_p),
+        ("best_sol", ctypes.c_void_p),
+    ]
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("max_bytes", ctypes.c_int64), ("round_ms", ctypes.c_double),
+                ("plain_min_pairs", ctypes.c_int64), ("reserved", ctypes.c_int32 * 8)]
+
+
+class Served(ctypes.Structure):
+    _fields_ = [
+        ("ticket", ctypes.c_int64), ("status", ctypes.c_int32), ("executor", ctypes.c_int32),
+        ("kind", ctypes.c_int32), ("pad", ctypes.c_int32), ("result", Result),
+        ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+        ("footprint_bytes", ctypes.c_int64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("admitted", ctypes.c_int64), ("completed", ctypes.c_int64),
+        ("queued", ctypes.c_int64), ("active", ctypes.c_int64), ("rounds", ctypes.c_int64),
+        ("bytes_in_use", ctypes.c_int64), ("bytes_budget", ctypes.c_int64), ("busy_s", ctypes.c_double),
     ]
 
 
@@ -167,6 +200,18 @@ def lib():
     L.ts_batch_destroy.argtypes = [P]
     L.ts_batch_run.restype = st
     L.ts_batch_run.argtypes = [P, I32, ctypes.POINTER(BatchOpts), P, P]
+    L.ts_server_create.restype = st
+    L.ts_server_create.argtypes = [ctypes.POINTER(ServerOpts), ctypes.POINTER(P)]
+    L.ts_server_submit.restype = st
+    L.ts_server_submit.argtypes = [P, ctypes.POINTER(Request), ctypes.POINTER(I64)]
+    L.ts_server_poll.restype = st
+    L.ts_server_poll.argtypes = [P, P, I32, ctypes.POINTER(I32), I32]
+    L.ts_server_stats_get.restype = st
+    L.ts_server_stats_get.argtypes = [P, ctypes.POINTER(ServerStats)]
+    L.ts_server_now.restype = ctypes.c_double
+    L.ts_server_now.argtypes = [P]
+    L.ts_server_destroy.restype = st
+    L.ts_server_destroy.argtypes = [P]
     _lib = L
     return L
 

@@ -365,3 +365,106 @@ def batch_solve(jobs, **kw) -> list[SolveResult]:
         return b.run()
     finally:
         b.close()
+
+
+@dataclass
+class Served:
+    """A completed request: its result, best solution and server-clock times (s)."""
+    ticket: int
+    status: int
+    executor: str
+    kind: int
+    result: SolveResult | None
+    submit_s: float
+    admit_s: float
+    done_s: float
+    footprint_bytes: int
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.submit_s
+
+
+class Server:
+    """Request loop with continuous batching (ts_server_*).
+
+    ``submit`` copies the request's edge list and returns a ticket; ``poll``
+    returns completed requests.  Each result equals the plain solver's on the
+    same graph and parameters."""
+
+    def __init__(self, *, max_bytes: int = 0, round_ms: float = 0.0, plain_min_pairs: int = 0):
+        o = C.ServerOpts()
+        o.max_bytes = max_bytes
+        o.round_ms = round_ms
+        o.plain_min_pairs = plain_min_pairs
+        h = ctypes.c_void_p()
+        C.check(C.lib().ts_server_create(ctypes.byref(o), ctypes.byref(h)), "ts_server_create")
+        self._h = h
+        self._pending = {}  # ticket -> (best array, problem)
+
+    def submit(self, n: int, u, v, w, problem: int, *, kind=-1, drop_self_loops=None, m: int = 0,
+               max_iter: int = 1000, tenure_policy: int = C.TENURE_FIXED, tenure: int = 20,
+               maxt: int = 200, piter: int = 500, gamma: int = 150, seed: int = 1, initial=None) -> int:
+        u = np.ascontiguousarray(u, dtype=np.int32)
+        v = np.ascontiguousarray(v, dtype=np.int32)
+        w = np.ascontiguousarray(w, dtype=np.int32)
+        p = default_params(problem)
+        p.m = m
+        p.max_iter = max_iter
+        p.tenure_policy = tenure_policy
+        p.tenure = tenure
+        p.maxt = maxt
+        p.piter = piter
+        p.gamma = gamma
+        p.seed = seed & 0xFFFFFFFF
+        q = C.Request()
+        q.n = n
+        q.num_edges = len(u)
+        q.u, q.v, q.w = u.ctypes.data, v.ctypes.data, w.ctypes.data
+        q.kind = -1 if kind is None or kind == -1 else struct_id(kind)
+        q.drop_self_loops = int(problem == C.PROBLEM_MDP) if drop_self_loops is None else int(drop_self_loops)
+        q.params = p
+        init = None if initial is None else np.ascontiguousarray(initial, dtype=np.int32)
+        q.initial = None if init is None else init.ctypes.data
+        best = np.zeros(m if problem == C.PROBLEM_MDP else n, np.int32)
+        q.best_sol = best.ctypes.data
+        t = ctypes.c_int64(0)
+        C.check(C.lib().ts_server_submit(self._h, ctypes.byref(q), ctypes.byref(t)), "ts_server_submit")
+        self._pending[t.value] = best
+        return t.value
+
+    def poll(self, wait_ms: int = 0, cap: int = 256) -> list[Served]:
+        buf = (C.Served * cap)()
+        got = ctypes.c_int32(0)
+        C.check(C.lib().ts_server_poll(self._h, buf, cap, ctypes.byref(got), int(wait_ms)), "ts_server_poll")
+        out = []
+        for k in range(got.value):
+            d = buf[k]
+            best = self._pending.pop(d.ticket, None)
+            r = d.result
+            res = None
+            if d.status == C.OK:
+                res = SolveResult(r.iterations, r.evaluations, r.cur, r.best, r.best_true, r.perturbations,
+                                  bool(r.stopped), best, r.device_error)
+            out.append(Served(d.ticket, d.status, "plain" if d.executor else "packed", d.kind, res,
+                              d.submit_s, d.admit_s, d.done_s, d.footprint_bytes))
+        return out
+
+    def now(self) -> float:
+        return C.lib().ts_server_now(self._h)
+
+    def stats(self) -> C.ServerStats:
+        s = C.ServerStats()
+        C.check(C.lib().ts_server_stats_get(self._h, ctypes.byref(s)), "ts_server_stats_get")
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            C.lib().ts_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
