@@ -243,7 +243,7 @@ ts_status build_packed(Req& r, int32_t kind) {
                            kind == S_WSWAP ? 4 * (int64_t)s.n_row_blocks * R * ldc : 0,
                            (int64_t)sizeof(KeyT) * m, (int64_t)sizeof(KeyT) * ldc, (int64_t)sizeof(DevState),
                            8 * s.log_cap, 8 * std::max<int64_t>(1, events * r.num_pert),
-                           4 * (int64_t)std::max<size_t>(1, r.initial.size()), (int64_t)sizeof(BatchResultDev),
+                           4 * (int64_t)(r.p.problem == P_MDP ? m : n), (int64_t)sizeof(BatchResultDev),
                            4 * (int64_t)(r.p.problem == P_MDP ? m : n)};
   int64_t total = 0;
   for (int64_t x : sizes) total += pad(x);
@@ -292,6 +292,10 @@ ts_status build_packed(Req& r, int32_t kind) {
     for (int64_t e = 0; e < events; e++) draw_event(rng, s.P, r.num_pert, draws);
   }
   cudaStream_t st = r.stream;
+  if ((int64_t)init.size() * 4 != sizes[12] || (int64_t)draws.size() * 8 > sizes[11]) {
+    set_error("ts_server: start or draw sizes do not match the solve");
+    return TS_ERR_INVALID_ARG;
+  }
   TS_CUDA(cudaMemcpyAsync(r.d_init, init.data(), 4 * init.size(), cudaMemcpyHostToDevice, st));
   if (!draws.empty())
     TS_CUDA(cudaMemcpyAsync(ptrs[11], draws.data(), 8 * draws.size(), cudaMemcpyHostToDevice, st));
