@@ -117,6 +117,7 @@ WORKLOADS = {
     "config3": ("mdp", "config3: plain MDP, Chung-Lu n=200000 (exponent 2.3, mean degree 50, max 5000), "
                        "m=2000, tenure 100"),
     "config1": ("mdp", "config1: plain MDP, Erdos-Renyi n=2000 mean degree 20, m=200, tenure 20"),
+    "config5": ("mixed", "config5: served"),
 }
 
 
@@ -320,6 +321,7 @@ def run_ours(args):
     if rank == 0:
         e2e = None if args.no_extras else run_e2e(T, torch, wl, kinds, args, seed, problem, m)
         cpu = None if args.no_extras else cpu_baseline_sample(wl, problem, m)
+        batched = None if (args.no_extras or args.no_batched) else run_batched(T, torch, dev, args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps, "higher_is_better": True,
@@ -333,6 +335,7 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
             "gpu_launches": len(kinds) * args.steps,
             "clocks": clocks.summary(),
             "wall_s_timed_region": wall,
@@ -349,12 +352,11 @@ def run_ours(args):
 
 
 def _hash_cap(deg: int) -> int:
-    cap = 1
-    while cap < deg:
+    """Slots of a vertex's hash table: power of two >= 4 * degree, at least 8."""
+    cap = 8
+    while cap < 4 * deg:
         cap <<= 1
-    if cap and deg / cap > 0.6:
-        cap <<= 1
-    return max(cap, 2)
+    return cap
 
 
 def run_e2e(T, torch, wl, kinds, args, seed, problem, m):
@@ -387,6 +389,196 @@ def run_e2e(T, torch, wl, kinds, args, seed, problem, m):
                     "ts_solver_step(steps) + ts_solver_result, wall clock"}
 
 
+def run_batched(T, torch, dev, args):
+    """Batched form on a bounded prefix of the batched workload (config 4):
+    `c4_instances` of its 4096 instances x 8 seeded restarts, 5000 iterations
+    each, structure and cluster size per size bucket from the autotuner.
+    value: solves per second of device time of one replay of the captured
+    launch (inputs resident); e2e: the same through the public API from
+    pinned host edge lists (graph builds, batch set-up, replay, results read
+    back); plain: a stratified sample of the same solves run one at a time
+    with ts_solver_* (init, step, result), wall clock; every sampled solve is
+    checked equal to its batched result."""
+    from ts_b200 import autotune as AT
+    t_tune = time.time()
+    table = AT.autotune(budget_s=args.tune_budget)
+    t_tune = time.time() - t_tune
+    insts = T.gen.config4(instances=args.c4_instances, restarts=8, iters=5000)
+    stream = torch.cuda.Stream(device=dev)
+    pinned = []
+    for inst in insts:
+        pinned.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+                       for a in (inst["u"], inst["v"], inst["w"])])
+    torch.cuda.synchronize(dev)
+    e2e0 = time.time()
+    graphs, specs = [], []
+    for inst, (u, v, w) in zip(insts, pinned):
+        mdp = inst["problem"] == "mdp"
+        prob = T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS
+        kind, cs = table.pick(prob, inst["n"])
+        g = T.Graph(inst["n"], u, v, w, kind, drop_self_loops=mdp)
+        graphs.append(g)
+        for sd in inst["seeds"]:
+            specs.append(T.BatchJobSpec(g, prob, m=inst["m"] if mdp else 0, max_iter=inst["iters"],
+                                        tenure_policy=T.TENURE_FIXED, tenure=20 if mdp else 50,
+                                        piter=500, gamma=150, seed=sd, cluster=cs))
+    b = T.Batch(specs, stream=stream.cuda_stream)
+    b.launch()
+    b.sync()
+    res = b.results()
+    e2e = time.time() - e2e0
+    info = b.info()
+    # device-timed replay
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    b.launch()
+    ev1.record(stream)
+    b.sync()
+    torch.cuda.synchronize(dev)
+    dev_s = ev0.elapsed_time(ev1) / 1e3
+    again = b.results()
+    assert all((a.best, a.best_true, a.iterations) == (c.best, c.best_true, c.iterations) for a, c in zip(res, again))
+    pairs = sum(((sp.m if sp.problem == T.PROBLEM_MDP else sp.graph.n // 2)
+                 * (sp.graph.n - (sp.m if sp.problem == T.PROBLEM_MDP else sp.graph.n // 2)) * r.iterations)
+                for sp, r in zip(specs, res))
+    # plain one-launch-per-iteration mode on a stratified sample (by work)
+    order = sorted(range(len(specs)), key=lambda q: res[q].evaluations)
+    stride = max(1, len(order) // args.c4_plain_sample)
+    sample = order[stride // 2::stride][:args.c4_plain_sample]
+    t_plain = 0.0
+    identical = True
+    for q in sample:
+        sp = specs[q]
+        t0 = time.time()
+        sv = T.Solver(sp.graph, sp.problem, m=sp.m, max_iter=sp.max_iter, tenure_policy=sp.tenure_policy,
+                      tenure=sp.tenure, piter=sp.piter, gamma=sp.gamma, seed=sp.seed)
+        sv.init(None)
+        sv.step(sp.max_iter)
+        r = sv.result()
+        sv.close()
+        t_plain += time.time() - t0
+        a = res[q]
+        identical &= (r.iterations, r.evaluations, r.cur, r.best, r.best_true) == \
+            (a.iterations, a.evaluations, a.cur, a.best, a.best_true) and bool(np.array_equal(r.best_sol, a.best_sol))
+    # the sample is stratified over the sorted work, so its mean time per solve
+    # estimates the mean over all solves
+    plain_sps = len(sample) / t_plain
+    b.close()
+    for g in graphs:
+        g.close()
+    sizes = [i["n"] for i in insts]
+    return {
+        "workload": f"config4 prefix: {len(insts)} of 4096 instances x 8 restarts = {len(specs)} solves; "
+                    "ER n log-uniform [200,20000], mean degree U[5,50], half MDP (m=U[5%,20%]n, tenure 20), "
+                    "half MaxBS (tenure 50, Piter 500, gamma 150); 5000 iterations each",
+        "solves": len(specs), "n_range": [min(sizes), max(sizes)],
+        "solves_per_s": len(specs) / dev_s, "device_s": dev_s, "swap_gains_per_s": pairs / dev_s,
+        "e2e_solves_per_s": len(specs) / e2e, "e2e_s": e2e,
+        "plain_solves_per_s": plain_sps, "plain_sample": len(sample),
+        "speedup_vs_plain": (len(specs) / dev_s) / plain_sps,
+        "e2e_speedup_vs_plain": (len(specs) / e2e) / plain_sps,
+        "identical_to_plain": bool(identical),
+        "groups": info.groups, "slots": info.slots, "slot_bytes": info.slot_bytes,
+        "autotune": table.as_dict(), "autotune_s": t_tune,
+    }
+
+
+def run_served(args):
+    """Served workload (config 5): open-loop Poisson arrivals at `rate`/s for
+    `duration` s; 70% MDP (Chung-Lu graphs) / 30% Max Bisection (conflict
+    graphs), n log-uniform in [1e3, 2e5], budgets U[1000, 10000] iterations.
+    The server builds each graph on the device from the request's host edge
+    list, admits by HBM footprint and batches solves continuously.  Beside it,
+    the plain one-at-a-time loop: the same requests each run alone (graph
+    build + ts_solver_*), queued FIFO at the same arrival times."""
+    import torch
+    import ts_b200 as T
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(55)
+    arrivals = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t > args.duration:
+            break
+        arrivals.append(t)
+    t_gen = time.time()
+    reqs = T.gen.config5_requests(len(arrivals), n_hi=args.served_n_hi)
+    t_gen = time.time() - t_gen
+    srv = T.Server(round_ms=args.round_ms)
+    got = {}
+    tickets = []
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = srv.now()
+    k = 0
+    while k < len(reqs) or len(got) < len(reqs):
+        now = srv.now() - t0
+        while k < len(reqs) and arrivals[k] <= now:
+            r = reqs[k]
+            mdp = r["problem"] == "mdp"
+            tk = srv.submit(r["n"], r["u"], r["v"], r["w"], T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS,
+                            kind="csr", m=r["m"] if mdp else 0, max_iter=r["iters"],
+                            tenure_policy=T.TENURE_FIXED, tenure=r["tenure"], seed=r["seed"])
+            tickets.append(tk)
+            k += 1
+        wait = 1 if k < len(reqs) else 20
+        for d in srv.poll(wait_ms=wait):
+            got[d.ticket] = d
+    clocks.stop()
+    st = srv.stats()
+    srv.close()
+    lat = np.array([got[tk].done_s - got[tk].submit_s for tk in tickets])
+    span = max(got[tk].done_s for tk in tickets) - t0
+    # plain one-at-a-time loop, FIFO at the same arrivals
+    service, identical = [], True
+    for tk, r in zip(tickets, reqs):
+        mdp = r["problem"] == "mdp"
+        torch.cuda.synchronize()
+        a = time.time()
+        g = T.Graph(r["n"], r["u"], r["v"], r["w"], "csr", drop_self_loops=mdp)
+        sv = T.Solver(g, T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS, m=r["m"] if mdp else 0, max_iter=r["iters"],
+                      tenure_policy=T.TENURE_FIXED, tenure=r["tenure"], seed=r["seed"])
+        sv.init(None)
+        sv.step(r["iters"])
+        res = sv.result()
+        sv.close()
+        g.close()
+        service.append(time.time() - a)
+        d = got[tk].result
+        identical &= d is not None and (d.best, d.best_true, d.iterations, d.evaluations) == \
+            (res.best, res.best_true, res.iterations, res.evaluations) and bool(np.array_equal(d.best_sol, res.best_sol))
+    fin, plain_lat = 0.0, []
+    for arr, sv_t in zip(arrivals, service):
+        fin = max(arr, fin) + sv_t
+        plain_lat.append(fin - arr)
+    plain_lat = np.array(plain_lat)
+    pct = lambda x, q: float(np.percentile(x, q))
+    line = {
+        "metric": METRIC, "value": len(tickets) / span, "unit": "solves/s", "n_gpus": 1,
+        "steps": len(tickets), "warmup": 0, "ms_per_step": 1e3 * span / len(tickets), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded per request)",
+        "config": {"workload": f"config5: Poisson arrivals {args.rate}/s for {args.duration} s; 70% MDP Chung-Lu "
+                               f"(m=n/100, tenure 100) / 30% MaxBS conflict (tenure 50); n log-uniform "
+                               f"[1000,{args.served_n_hi}]; budgets U[1000,10000]; structure csr",
+                   "round_ms": args.round_ms},
+        "served": {"requests": len(tickets), "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95),
+                                                           "p99": pct(lat, 99), "max": float(lat.max())},
+                   "executors": {e: sum(1 for tk in tickets if got[tk].executor == e) for e in ("packed", "plain")},
+                   "rounds": st.rounds, "busy_s": st.busy_s, "span_s": span},
+        "plain_one_at_a_time": {"solves_per_s": len(tickets) / (fin - arrivals[0] + arrivals[0]),
+                                "latency_s": {"p50": pct(plain_lat, 50), "p95": pct(plain_lat, 95),
+                                              "p99": pct(plain_lat, 99), "max": float(plain_lat.max())},
+                                "service_s_total": float(sum(service))},
+        "identical_to_alone": bool(identical),
+        "generation_s": t_gen,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -396,12 +588,22 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 is the benchmark; the others serve profiling")
     ap.add_argument("--structures", default="", help="comma list (default: all six)")
-    ap.add_argument("--no-extras", action="store_true", help="skip the e2e and CPU-baseline legs")
+    ap.add_argument("--no-extras", action="store_true", help="skip the e2e, CPU-baseline and batched legs")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (config 4) leg")
+    ap.add_argument("--c4-instances", type=int, default=40, help="batched leg: instances of config 4")
+    ap.add_argument("--c4-plain-sample", type=int, default=24, help="batched leg: solves run plain")
+    ap.add_argument("--tune-budget", type=float, default=30.0, help="autotuner time budget (s)")
+    ap.add_argument("--rate", type=float, default=2.0, help="config5: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="config5: arrival window (s)")
+    ap.add_argument("--served-n-hi", type=int, default=200_000, help="config5: largest n")
+    ap.add_argument("--round-ms", type=float, default=5.0, help="config5: server round target")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "config5":
+        return run_served(args)
     return run_ours(args)
 
 

@@ -228,3 +228,62 @@ def config3(n: int = 200_000, seed: int = 3):
     """MDP large: Chung-Lu n=200k, exponent 2.3, mean 50, max 5000; m=2000, tenure 100, 500 iterations."""
     u, v, w, _ = chung_lu(n, 2.3, 50.0, 5000, seed=seed)
     return dict(n=n, u=u, v=v, w=w, m=2000 if n >= 200_000 else max(2, n // 100), tenure=100, iters=500)
+
+
+def _mix(*xs: int) -> int:
+    """Deterministic 32-bit hash of a few integers (splitmix64 finaliser)."""
+    h = 0x9E3779B97F4A7C15
+    for x in xs:
+        h = (h ^ (x + 0x9E3779B97F4A7C15 + (h << 6) + (h >> 2))) & 0xFFFFFFFFFFFFFFFF
+        h ^= h >> 30
+        h = (h * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        h ^= h >> 27
+        h = (h * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        h ^= h >> 31
+    return int(h & 0x7FFFFFFF) or 1
+
+
+def config4(instances: int = 4096, restarts: int = 8, iters: int = 5000, seed: int = 4,
+            n_lo: int = 200, n_hi: int = 20000, first: int = 0):
+    """Batched workload: `instances` Erdos-Renyi instances with n log-uniform in
+    [n_lo, n_hi], mean degree U[5, 50], node weights U[1,1000]; even instances
+    MDP with m = U[5%, 20%] n, odd ones Max Bisection; `restarts` seeded solves
+    each (seed = hash(instance, restart)); `iters` iterations per solve.
+    Instances [first, first + instances) of the sequence, so a bounded sample
+    is a prefix of the full workload."""
+    rng = np.random.default_rng(seed)
+    out = []
+    total = first + instances
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=total)).astype(np.int64)
+    degs = rng.uniform(5, 50, size=total)
+    fr = rng.uniform(0.05, 0.20, size=total)
+    for i in range(first, total):
+        n = int(ns[i])
+        u, v, w, _ = erdos_renyi(n, float(min(degs[i], n - 1)), _mix(seed, i))
+        mdp = i % 2 == 0
+        out.append(dict(index=i, n=n, u=u, v=v, w=w, problem="mdp" if mdp else "maxbs",
+                        m=max(1, int(round(fr[i] * n))) if mdp else n // 2,
+                        seeds=[_mix(i, r) for r in range(restarts)], iters=iters))
+    return out
+
+
+def config5_requests(count: int, seed: int = 5, n_lo: int = 1000, n_hi: int = 200_000):
+    """Served workload requests: 70% MDP (Chung-Lu graph as config 3, m = n/100,
+    tenure 100), 30% Max Bisection (conflict graph as config 2, tenure 50);
+    n log-uniform in [n_lo, n_hi]; iteration budget U[1000, 10000]; every
+    graph from a per-request seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+        mdp = rng.random() < 0.7
+        iters = int(rng.integers(1000, 10001))
+        s = _mix(seed, i)
+        if mdp:
+            u, v, w, _ = chung_lu(n, 2.3, 50.0, min(5000, n - 1), s)
+            out.append(dict(n=n, u=u, v=v, w=w, problem="mdp", m=max(2, n // 100), tenure=100,
+                            iters=iters, seed=s))
+        else:
+            u, v, w, _ = conflict_graph(n, 60.0, max(1, 2000 * n // 100_000), 8, 32, s)
+            out.append(dict(n=n, u=u, v=v, w=w, problem="maxbs", m=n // 2, tenure=50, iters=iters, seed=s))
+    return out
