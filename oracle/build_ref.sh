@@ -38,3 +38,11 @@ for p in "mdp GPU-MDP mdp" "maxbisection GPU-MAXBS maxbs"; do
   done
 done
 } | xargs -P 6 -L 1 bash -c 'build_one "$0" "$1" "$2" "$3" "$4"'
+# the reference's instance converter (host C++, one source file)
+if [ ! "$OUT/convert_mwis" -nt "$REF/src/convert_mwis.cpp" ]; then
+  if g++ -O2 -std=c++17 "$REF/src/convert_mwis.cpp" -o "$OUT/convert_mwis" > "$OUT/convert_mwis.build.log" 2>&1; then
+    echo "built $OUT/convert_mwis"
+  else
+    echo "NOT BUILDABLE: $REF/src/convert_mwis.cpp"
+  fi
+fi

@@ -17,7 +17,7 @@ def run(args, **kw):
 
 @pytest.fixture(scope="module", autouse=True)
 def built():
-    if not os.path.exists(os.path.join(BIN, "mdp_csr")):
+    if not all(os.path.exists(os.path.join(BIN, b)) for b in ("mdp_csr", "maxbs_csr", "convert_mwis")):
         subprocess.run(["make", "-s", "-C", PKG, "cli"], check=True)
 
 
@@ -116,3 +116,65 @@ def test_runner_resume_marker_and_layout(tmp_path):
     with pytest.raises(ValueError):
         R.quantidade_vertices(g)
     assert R.ALGOS["csr-bb"] == "CSR-BuscaBinaria"
+
+
+def _mwis_fixture(root, name, n, edges, weights):
+    d = root / name
+    d.mkdir(parents=True)
+    (d / "conflict_graph.txt").write_text(f"{n} {len(edges)}\n" + "".join(f"{a} {b}\n" for a, b in edges))
+    (d / "node_weights.txt").write_text("".join(f"{v} {wt}\n" for v, wt in weights))
+
+
+def test_converter_known_answer(tmp_path):
+    inp, out = tmp_path / "in", tmp_path / "out"
+    # duplicates in both orientations, a negative weight sum, sums >= 1000
+    _mwis_fixture(inp, "tiny", 4, [(2, 1), (1, 2), (3, 4), (4, 1), (3, 4), (1, 3)],
+                  [(1, 1500), (2, 7), (3, -20), (4, 999)])
+    r = run([os.path.join(BIN, "convert_mwis"), str(inp), str(out), "tiny"])
+    assert r.returncode == 0, r.stderr
+    assert "2 duplicatas removidas" in r.stdout
+    assert (out / "tiny.txt").read_text() == (
+        "4 4 4\n"
+        "1 2 1.507\n"
+        "1 3 1.480\n"
+        "1 4 2.499\n"
+        "3 4 0.979\n")
+    _mwis_fixture(inp, "neg", 2, [(1, 2)], [(1, -1500), (2, -7)])
+    r = run([os.path.join(BIN, "convert_mwis"), str(inp), str(out), "neg"])
+    assert (out / "neg.txt").read_text() == "2 2 1\n1 2 -1.507\n"
+
+
+def test_converter_errors(tmp_path):
+    inp, out = tmp_path / "in", tmp_path / "out"
+    _mwis_fixture(inp, "bad", 3, [(1, 4)], [(1, 1), (2, 2), (3, 3)])
+    r = run([os.path.join(BIN, "convert_mwis"), str(inp), str(out), "bad"])
+    assert r.returncode == 1 and "invalida" in r.stderr
+    r = run([os.path.join(BIN, "convert_mwis")])
+    assert r.returncode == 1 and "Uso:" in r.stderr
+
+
+REF_CONVERTER = os.path.join(os.path.dirname(PKG), "oracle", "_ref", "convert_mwis")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CONVERTER), reason="reference converter not built (oracle/build_ref.sh)")
+def test_converter_matches_reference_converter(tmp_path):
+    import numpy as np
+    rng = np.random.default_rng(8)
+    inp = tmp_path / "in"
+    names = []
+    for k in range(4):
+        n = int(rng.integers(5, 400))
+        m = int(rng.integers(1, 3 * n))
+        a = rng.integers(1, n + 1, size=m)
+        b = rng.integers(1, n + 1, size=m)
+        keep = a != b
+        edges = list(zip(a[keep].tolist(), b[keep].tolist()))
+        edges += edges[: len(edges) // 4]  # duplicates
+        wts = rng.integers(-5000, 10**9, size=n)
+        _mwis_fixture(inp, f"i{k}", n, edges, [(v + 1, int(wts[v])) for v in range(n)])
+        names.append(f"i{k}")
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    assert run([os.path.join(BIN, "convert_mwis"), str(inp), str(ours)]).returncode == 0
+    assert run([REF_CONVERTER, str(inp), str(ref)]).returncode == 0
+    for nm in names:
+        assert (ours / f"{nm}.txt").read_bytes() == (ref / f"{nm}.txt").read_bytes(), nm
