@@ -111,6 +111,7 @@ __device__ void slot_init(const DevGraph& g, const DevSolver<KeyT>& s, const int
     z.cur = obj;
     z.best = obj;
     z.target = max_iter;
+    z.pert_limit = s.draw_events;  // every event of the solve is staged
     *s.st = z;
   }
   __syncthreads();
@@ -193,7 +194,9 @@ __device__ void cluster_iterate(const DevGraph& g, const DevSolver<KeyT>& s, lon
     long long k = LLONG_MIN, i = LLONG_MAX;
     for (int t = (int)rank; t < ntiles; t += (int)cs) {
       long long tk, ti;
-      tile_eval<PROB, ST, KeyT, true>(g, s, mode, it, D64, t / s.n_chunks, t % s.n_chunks, tk, ti, sh);
+      // k (valid in thread 0, the thread that uses it): the CTA's best so far
+      tile_eval<PROB, ST, KeyT, true>(g, s, mode, it, D64, t / s.n_chunks, t % s.n_chunks, tk, ti, sh,
+                                      mode == 0 ? k : LLONG_MIN);
       if (tid == 0) better_rec(k, i, tk, ti);
     }
     if (tid == 0) { s_rec.key = k; s_rec.idx = i; }

@@ -334,6 +334,7 @@ ts_status prepare_draws(ts_solver* s, int64_t iters_ahead) {
   TS_CUDA(cudaMemcpyAsync(s->draws.p, s->host_draws.data() + consumed * k,
                           sizeof(long long) * need * k, cudaMemcpyHostToDevice, s->g->stream));
   s->h_st->pert_base = consumed;
+  s->h_st->pert_limit = need;
   return TS_OK;
 }
 

@@ -444,11 +444,15 @@ __device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mo
   __syncthreads();
   if (PROB == P_MAXBS && sh.action == 3) {
     const long long ev = st->pert_events - st->pert_base;
-    if (ev < 0 || ev >= s.draw_events) {
+    if (ev < 0 || ev >= s.draw_events || ev >= st->pert_limit) {
       if (threadIdx.x == 0) { st->err |= E_PERTURB_WINDOW; st->done = 1; }
     } else {
       for (int32_t q = 0; q < s.num_pert; q++) {
         const long long mv = s.draws[ev * s.num_pert + q];
+        if (mv < 0 || mv >= s.P) {  // never index with a bad draw (the same value in every thread)
+          if (threadIdx.x == 0) { st->err |= E_BAD_INDEX; st->done = 1; }
+          break;
+        }
         const int32_t pu = (int32_t)(mv / s.delta), pv = (int32_t)(mv % s.delta);
         const long long aux = apply_swap<PROB, ST, KeyT>(g, s, pu, pv, iter + 1, 0, 0, false, sh);
         if (threadIdx.x == 0) {
@@ -472,11 +476,13 @@ __device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mo
 // pass (mode 0), or best pair under the full reference key rule (mode 1);
 // (out_key, out_idx) valid in thread 0, (LLONG_MIN, LLONG_MAX) if none.
 // Used once per CTA by the plain kernel and in a loop by the batched one
-// (PERSIST: state written earlier in the same launch, see ld_st).
+// (PERSIST: state written earlier in the same launch, see ld_st).  floor_key:
+// the best key the caller holds from earlier tiles; a tile whose maximum is
+// below it returns no record.
 template <int PROB, int ST, class KeyT, bool PERSIST>
 __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
                           long long D64, int rb, int ch, long long& out_key, long long& out_idx,
-                          TailShared& sh) {
+                          TailShared& sh, long long floor_key = LLONG_MIN) {
   constexpr int R = Rows<ST>::R;
   constexpr int TPB = Tpb<ST>::v;
   using Lim = KeyLim<KeyT>;
@@ -849,7 +855,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         if ((long long)v > mc) { mc = (long long)v; rstar = r; }
       }
       s_mc = mc;
-      s_rstar = rstar;
+      // A tile whose maximum is below what the caller already holds cannot
+      // win the iteration: skip its rescan.
+      s_rstar = mc < floor_key ? -1 : rstar;
       s_cmin = 0xffffffffu;
     }
     __syncthreads();

@@ -71,6 +71,7 @@ struct DevState {
   long long trace_n;
   long long pert_events;  // perturbation events consumed
   long long pert_base;    // first event held in the device draw window
+  long long pert_limit;   // events of the window that hold draws (from pert_base)
   long long pert_moves;
   unsigned int counter;   // last-CTA-done ticket
   int32_t mode;           // 0 fast sweep, 1 exact sweep

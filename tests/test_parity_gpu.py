@@ -237,3 +237,45 @@ def test_int64_keys(gpu, kind):
                 tenure=9, seed=2)
     compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=150, tenure_policy=T.TENURE_FIXED,
                 tenure=9, piter=20, gamma=10, seed=2)
+
+
+@pytest.mark.parametrize("kind", ["csr", "hash", "csr-bitset-bb"])
+def test_caller_supplied_perturbation_stream(gpu, kind):
+    # ts_solver_set_perturbations: the search uses the caller's events, here the
+    # stream of another seed; the oracle with that seed must agree move for move
+    n = 160
+    u, v, w = node_weight_graph(n, 7.0, 21)
+    part = np.ones(n, np.int32)
+    part[np.arange(0, n, 2)] = 0
+    iters, piter, gamma = 400, 15, 16
+    events = iters // piter + 1
+    draws = T.perturb_draws(n, 99, gamma, False, events)
+    og = O.Graph(n, u, v, w, drop_self_loops=False)
+    o = O.run(og, O.MAXBS, max_iter=iters, tenure_policy=T.TENURE_FIXED, tenure=12, piter=piter, gamma=gamma,
+              seed=99, initial=part, threads=0)
+    g = T.Graph(n, u, v, w, kind, drop_self_loops=False)
+    s = T.Solver(g, T.PROBLEM_MAXBS, max_iter=iters, tenure_policy=T.TENURE_FIXED, tenure=12, piter=piter,
+                 gamma=gamma, seed=5, trace=True)
+    try:
+        s.init(part)
+        s.set_perturbations(draws)
+        s.step(iters)
+        tr = s.trace()
+        r = s.result()
+        assert (o.trace["kind"] == O.REC_PERTURB).any()
+        for f in ("iter", "idx", "key", "cur", "best", "kind"):
+            np.testing.assert_array_equal(tr[f], o.trace[f])
+        assert (r.best, r.best_true, r.cur) == (o.best, o.best_true, o.cur)
+        # too few events: the search stops with a device error instead of inventing moves
+        s.init(part)
+        s.set_perturbations(draws[:1])
+        with pytest.raises(T.TsError) as ei:
+            s.step(iters)
+        assert ei.value.status == 5
+        s.init(part)
+        s.step(1)
+        with pytest.raises(T.TsError):
+            s.set_perturbations(draws)  # only before the first step
+    finally:
+        s.close()
+        g.close()
