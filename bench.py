@@ -121,9 +121,9 @@ WORKLOADS = {
 }
 
 
-def build_workload(name: str = "config2"):
+def build_workload(name: str = "config2", n: int = 0):
     from ts_b200 import gen
-    wl = getattr(gen, name)()
+    wl = getattr(gen, name)(n) if n else getattr(gen, name)()
     wl["problem"], wl["desc"] = WORKLOADS[name]
     return wl
 
@@ -227,7 +227,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
-    wl = build_workload(args.workload)
+    wl = build_workload(args.workload, args.n)
     n, u, v, w = wl["n"], wl["u"], wl["v"], wl["w"]
     mdp = wl["problem"] == "mdp"
     problem = T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS
@@ -590,6 +590,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config2",
                     help="config2 is the benchmark; the others serve profiling")
     ap.add_argument("--structures", default="", help="comma list (default: all six)")
+    ap.add_argument("--n", type=int, default=0, help="config2/config3 at another size (profiling cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, CPU-baseline and batched legs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (config 4) leg")
     ap.add_argument("--c4-instances", type=int, default=40, help="batched leg: instances of config 4")
