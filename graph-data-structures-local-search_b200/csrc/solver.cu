@@ -494,7 +494,11 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   int64_t max_cols = full;
   if (g->kind == S_WSWAP) max_cols = 8 * pc;
   if (mdp_csr) max_cols = 16 * pc;
-  const int64_t min_grid = g->kind == S_WSWAP ? 4 * 148 : 2 * 148;
+  // Tiles per iteration: the staged structures (per-tile row staging, uneven
+  // rows) balance better over many column chunks; CSR and WSwap prefer few
+  // wide tiles.  One CTA per tile; the hardware schedules them.
+  const bool staged = g->kind != S_CSR && g->kind != S_WSWAP;
+  const int64_t min_grid = staged ? 8 * 148 : (g->kind == S_WSWAP ? 4 * 148 : 2 * 148);
   const int64_t want_chunks = std::max<int64_t>(1, (min_grid + s->n_row_blocks - 1) / s->n_row_blocks);
   int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
   cols = ((cols + pc - 1) / pc) * pc;
