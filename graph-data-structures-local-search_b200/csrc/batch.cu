@@ -278,8 +278,7 @@ ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_b
   }
   G.smem = smem;
   auto kern = batch_kernel<PROB, ST, KeyT>;
-  if (smem > 48 * 1024)
-    TS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TS_CUDA(allow_dyn_smem(reinterpret_cast<const void*>(kern), smem));
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = cs;

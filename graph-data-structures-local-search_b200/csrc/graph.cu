@@ -16,6 +16,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "ts_host.h"
@@ -32,6 +33,17 @@ ts_status cuda_fail(cudaError_t e, const char* what) {
   set_error(m);
   cudaGetLastError();  // clear sticky-free errors
   return e == cudaErrorMemoryAllocation ? TS_ERR_OUT_OF_MEMORY : TS_ERR_CUDA;
+}
+
+cudaError_t allow_dyn_smem(const void* fn, size_t smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= smem) return cudaSuccess;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 namespace {

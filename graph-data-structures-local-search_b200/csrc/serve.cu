@@ -78,12 +78,8 @@ serve_kernel(const ServeJobDev<KeyT>* __restrict__ jobs) {
 template <int PROB, int ST, class KeyT>
 cudaError_t launch_serve(cudaStream_t st, const void* jobs, int njobs, int cs, size_t smem) {
   auto kern = serve_kernel<PROB, ST, KeyT>;
-  static size_t attr = 48 * 1024;
-  if (smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = smem;
-  }
+  cudaError_t e = allow_dyn_smem(reinterpret_cast<const void*>(kern), smem);
+  if (e != cudaSuccess) return e;
   cudaLaunchAttribute a[1];
   a[0].id = cudaLaunchAttributeClusterDimension;
   a[0].val.clusterDim.x = cs;

@@ -196,12 +196,8 @@ template <int PROB, int ST, class KeyT>
 cudaError_t launch_iter(const DevGraph& g, const DevSolver<KeyT>& s, int grid, size_t smem,
                         cudaStream_t st, int count) {
   auto fn = iter_kernel<PROB, ST, KeyT>;
-  static size_t attr_bytes = 48 * 1024;  // per instantiation: largest opt-in so far
-  if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_bytes = smem;
-  }
+  cudaError_t e = allow_dyn_smem(reinterpret_cast<const void*>(fn), smem);
+  if (e != cudaSuccess) return e;
   for (int i = 0; i < count; i++) fn<<<grid, Tpb<ST>::v, smem, st>>>(g, s);
   return cudaGetLastError();
 }

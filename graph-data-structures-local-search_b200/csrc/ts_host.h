@@ -102,5 +102,9 @@ void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0
 void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out);
 // Dynamic shared memory for staging R rows of a lookup structure.
 int32_t staging_bytes(const ts_graph* g, int R);
+// Opts kernel `fn` in to `smem` bytes of dynamic shared memory on the current
+// device.  The limit only grows (under a lock), so a launch planned earlier
+// with a larger size stays valid when a smaller one is planned later.
+cudaError_t allow_dyn_smem(const void* fn, size_t smem);
 
 }  // namespace tsb

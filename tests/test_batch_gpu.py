@@ -230,3 +230,50 @@ def test_batch_rejects_bad_jobs(gpu):
             T.batch_solve([spec])
         assert ei.value.status == 1
     g.close()
+
+
+_SHARED_KERNEL_CHILD = r"""
+import sys
+import numpy as np
+sys.path[:0] = sys.argv[1:]
+import ts_b200 as T
+from test_batch_gpu import assert_same, plain
+
+def sparse(n, seed):
+    rng = np.random.default_rng(seed)
+    u = rng.integers(0, n, size=3 * n).astype(np.int32)
+    v = rng.integers(0, n, size=3 * n).astype(np.int32)
+    w = rng.integers(1, 1000, size=3 * n).astype(np.int32)
+    return u, v, w
+
+# MDP over CSR stages 4 bytes per column of a tile: n - m = 15000 and 13000
+# columns need 61440 and 53248 bytes of shared memory, both above the default
+# 48 KB, in the same kernel instantiation but in two groups (cluster 2 and 1).
+ga = T.Graph(16000, *sparse(16000, 1), "csr", drop_self_loops=True)
+gb = T.Graph(14000, *sparse(14000, 2), "csr", drop_self_loops=True)
+specs = [T.BatchJobSpec(ga, T.PROBLEM_MDP, m=1000, max_iter=60, seed=5, cluster=2),
+         T.BatchJobSpec(gb, T.PROBLEM_MDP, m=1000, max_iter=20, seed=6, cluster=1)]
+b = T.Batch(specs)
+assert b.info().groups == 2
+b.launch()
+b.sync()
+for q, (r, sp) in enumerate(zip(b.results(), specs)):
+    assert_same(r, plain(sp), f"job {q}")
+b.close()
+print("ok")
+"""
+
+
+def test_groups_sharing_a_kernel_with_different_shared_memory(gpu):
+    """Two groups of one kernel instantiation, the larger-staging one planned
+    first: planning the second must not lower the kernel's shared-memory
+    opt-in below what the first one's launch needs.  Runs in a fresh process
+    so no earlier test has raised the opt-in already."""
+    import os
+    import subprocess
+    import sys
+    from conftest import PKG, ROOT
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run([sys.executable, "-c", _SHARED_KERNEL_CHILD, here, PKG, ROOT],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-3000:]
