@@ -130,7 +130,10 @@ def build_workload(name: str = "config2", n: int = 0):
 
 def algorithmic_bytes(kind: str, n: int, m: int, ldc: int, key_bytes: int, deg_in: np.ndarray,
                       cap_in: np.ndarray, wpr: int) -> int:
-    """Compulsory HBM bytes of one iteration of `kind` (roofline)."""
+    """Compulsory HBM bytes of one iteration of `kind`: the row and column
+    state every structure reads (contributions, tabu stamps, vertex ids) plus
+    what its lookups must touch once -- the inside rows' CSR entries, hash
+    tables or bitmap rows, or the whole WSwap matrix."""
     delta = n - m
     base = m * (key_bytes + 8) + delta * (key_bytes + 4)  # row side: vg, tabu, id; columns: vg, tabu
     if kind == "csr":

@@ -215,6 +215,58 @@ cudaError_t launch_iter_st(int kind, const DevGraph& g, const DevSolver<KeyT>& s
   }
 }
 
+// Resident CTAs per SM of the WSwap iteration kernel.
+int wswap_blocks_per_sm(int problem, bool wide) {
+  int nb = 0;
+  cudaError_t e;
+  if (problem == P_MDP)
+    e = wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MDP, S_WSWAP, long long>,
+                                                             Tpb<S_WSWAP>::v, 16)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MDP, S_WSWAP, int32_t>,
+                                                             Tpb<S_WSWAP>::v, 16);
+  else
+    e = wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MAXBS, S_WSWAP, long long>,
+                                                             Tpb<S_WSWAP>::v, 16)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MAXBS, S_WSWAP, int32_t>,
+                                                             Tpb<S_WSWAP>::v, 16);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
+// Column split of a streamed sweep into whole waves: the matrix streams at full
+// bandwidth only while every resident CTA slot is busy, so among the splits
+// with at least one full wave of tiles (columns a multiple of pc, between lo
+// and cap) take the one whose last wave is fullest; near-ties go to more
+// tiles.  Returns `fallback` when no split fills a wave.
+int64_t wave_cols(int64_t delta, int64_t rows, int64_t pc, int64_t lo, int64_t cap, int64_t slots,
+                  int64_t fallback) {
+  if (slots <= 0 || rows <= 0) return fallback;
+  double best = -1.0;
+  int64_t pick = fallback, pick_tiles = 0;
+  const int64_t max_nc = (delta + pc - 1) / pc;
+  for (int64_t nc = 1; nc <= max_nc; nc++) {
+    const int64_t c = (((delta + nc - 1) / nc + pc - 1) / pc) * pc;
+    if (c > cap || c < lo) continue;
+    const int64_t tiles = rows * ((delta + c - 1) / c);
+    if (tiles < slots) continue;
+    const int64_t waves = (tiles + slots - 1) / slots;
+    const double eff = (double)rows * (double)delta / (double)c / ((double)waves * (double)slots);
+    if (eff > best + 0.005) {
+      best = eff;
+      pick = c;
+      pick_tiles = tiles;
+    } else if (eff >= best - 0.005 && tiles > pick_tiles) {
+      best = std::max(best, eff);
+      pick = c;
+      pick_tiles = tiles;
+    }
+  }
+  return pick;
+}
+
 int rows_per_tile(int kind) {
   switch (kind) {
     case S_CSR: return Rows<S_CSR>::R;
@@ -499,6 +551,12 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
   cols = ((cols + pc - 1) / pc) * pc;
   cols = std::max<int64_t>(pc, std::min<int64_t>(cols, max_cols));
+  if (g->kind == S_WSWAP) {
+    int sms = 0;
+    TS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    const int64_t slots = (int64_t)wswap_blocks_per_sm(p->problem, s->wide) * sms;
+    cols = wave_cols(s->delta, s->n_row_blocks, pc, 8 * pc, 64 * pc, slots, cols);
+  }
   s->chunk_cols = (int32_t)cols;
   s->n_chunks = (int32_t)((s->delta + cols - 1) / cols);
   s->grid = s->n_row_blocks * s->n_chunks;

@@ -295,35 +295,65 @@ __device__ long long apply_swap(const DevGraph& g, const DevSolver<KeyT>& s, int
   const int32_t nu = (int32_t)(g.rowptr[u + 1] - su), nv = (int32_t)(g.rowptr[v + 1] - sv);
   if (threadIdx.x == 0) sh.wuv = 0;
   __syncthreads();
-  for (int32_t k = threadIdx.x; k < nu + nv; k += blockDim.x) {
-    const bool from_u = k < nu;
-    const long long at = from_u ? su + k : sv + (k - nu);
-    const long long rs = from_u ? su : sv;
-    const int2 e = g.adj[at];
-    const int32_t z = e.x, w = e.y;
-    const int32_t p = s.pos[z];
-    KeyT d;
-    if (PROB == P_MDP) {
-      d = from_u ? -(KeyT)w : (KeyT)w;
-    } else {
-      const bool z_in = p < m;
-      d = (from_u == z_in) ? -(KeyT)2 * (KeyT)w : (KeyT)2 * (KeyT)w;
+  // The moved vertices' adjacency, kApplyBatch entries per thread in flight:
+  // every load of a batch is issued before any is used (a hub row of
+  // thousands of entries is a few dependent round trips, not one per 256
+  // entries).  The updates are integer atomics: their order does not matter.
+  // (One per thread for MaxBS WSwap, whose sweep would lose a resident CTA
+  // per SM to the extra registers.)
+  constexpr int kApplyBatch = (PROB == P_MAXBS && ST == S_WSWAP) ? 1 : 3;
+  const int32_t total = nu + nv;
+  for (int32_t base = 0; base < total; base += kApplyBatch * (int32_t)blockDim.x) {
+    int2 e[kApplyBatch];
+    int32_t prev[kApplyBatch];
+    long long rv[kApplyBatch];
+#pragma unroll
+    for (int j = 0; j < kApplyBatch; j++) {
+      const int32_t k = base + j * (int32_t)blockDim.x + (int32_t)threadIdx.x;
+      const bool from_u = k < nu;
+      const long long at = from_u ? su + k : sv + (k - nu);
+      const long long rs = from_u ? su : sv;
+      e[j] = make_int2(-1, 0);
+      prev[j] = -1;
+      rv[j] = 0;
+      if (k < total) {
+        e[j] = g.adj[at];
+        if (at != rs) prev[j] = g.adj[at - 1].x;
+        if (ST == S_CSR) rv[j] = g.rev[at];
+      }
     }
-    atomic_add_key(vg_at(s, p), d);
-    if (ST == S_CSR) s.cpos[g.rev[at]] = from_u ? m + jv : iu;  // new position of u / v
-    const bool first = at == rs || g.adj[at - 1].x != z;
-    if (PROB == P_MAXBS && from_u && z == v && first) sh.wuv = w;
-    if (ST == S_WSWAP && first && z != (from_u ? u : v)) {
-      // Row iu now describes v, column jv now describes u
-      // (updateVertexEdgeGain, GPU-MDP-WSwap.cu:535-560).  Self-loop entries
-      // (kept by the MaxBS loader) are skipped: the reference's patch would fold
-      // them into W[iu][jv], and W must keep returning the CSR lookup's w(u,v).
-      if (from_u && z != v) {
-        if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], -w);
-        else atomicAdd(&s.W[(long long)p * s.ldc + jv], w);
-      } else if (!from_u && z != u) {
-        if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], w);
-        else atomicAdd(&s.W[(long long)p * s.ldc + jv], -w);
+    int32_t pz[kApplyBatch];
+#pragma unroll
+    for (int j = 0; j < kApplyBatch; j++) pz[j] = e[j].x >= 0 ? s.pos[e[j].x] : 0;
+#pragma unroll
+    for (int j = 0; j < kApplyBatch; j++) {
+      const int32_t k = base + j * (int32_t)blockDim.x + (int32_t)threadIdx.x;
+      if (k >= total) continue;
+      const bool from_u = k < nu;
+      const int32_t z = e[j].x, w = e[j].y, p = pz[j];
+      KeyT d;
+      if (PROB == P_MDP) {
+        d = from_u ? -(KeyT)w : (KeyT)w;
+      } else {
+        const bool z_in = p < m;
+        d = (from_u == z_in) ? -(KeyT)2 * (KeyT)w : (KeyT)2 * (KeyT)w;
+      }
+      atomic_add_key(vg_at(s, p), d);
+      if (ST == S_CSR) s.cpos[rv[j]] = from_u ? m + jv : iu;  // new position of u / v
+      const bool first = prev[j] != z;
+      if (PROB == P_MAXBS && from_u && z == v && first) sh.wuv = w;
+      if (ST == S_WSWAP && first && z != (from_u ? u : v)) {
+        // Row iu now describes v, column jv now describes u
+        // (updateVertexEdgeGain, GPU-MDP-WSwap.cu:535-560).  Self-loop entries
+        // (kept by the MaxBS loader) are skipped: the reference's patch would fold
+        // them into W[iu][jv], and W must keep returning the CSR lookup's w(u,v).
+        if (from_u && z != v) {
+          if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], -w);
+          else atomicAdd(&s.W[(long long)p * s.ldc + jv], w);
+        } else if (!from_u && z != u) {
+          if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], w);
+          else atomicAdd(&s.W[(long long)p * s.ldc + jv], -w);
+        }
       }
     }
   }
@@ -931,8 +961,16 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
 // ------------------------------------------------------------------ kernel
 // Plain form: one launch = one iteration; CTA b evaluates tile b, the last
 // CTA to finish reduces the records and applies the move.
+// Minimum resident CTAs per SM the plain kernel is compiled for (0: left to
+// the compiler).  MDP WSwap with 32-bit keys is held to 64 registers so four
+// CTAs share an SM: the matrix stream is bound by loads in flight, and the
+// fourth CTA moves an n = 200,000, m = 2,000 sweep from 4.3 to 4.9 TB/s
+// (a few bytes of spills, outside the sweep loop, cost less than the lost CTA).
+template <int PROB, int ST, class KeyT> struct IterMinBlocks { static constexpr int v = 0; };
+template <> struct IterMinBlocks<P_MDP, S_WSWAP, int32_t> { static constexpr int v = 4; };
+
 template <int PROB, int ST, class KeyT>
-__global__ void __launch_bounds__(Tpb<ST>::v)
+__global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT>::v))
 iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   DevState* st = s.st;
   if (st->done || st->iter >= st->target) return;
