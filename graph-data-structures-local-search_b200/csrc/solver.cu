@@ -94,12 +94,13 @@ int32_t staging_bytes(const ts_graph* g, int R) {
   int64_t row_bytes = 2 * r16(4 * slots);
   if (g->kind == S_BB || g->kind == S_BITSET_BB) {  // + bucket directory
     int64_t nb = 16;
-    while (nb < d90 / 2 && nb < 4096) nb <<= 1;
+    while (nb < 2 * d90 && nb < 4096) nb <<= 1;
     row_bytes += r16(4 * (nb + 1));
   }
   if (g->kind == S_BITSET || g->kind == S_BITSET_BB) row_bytes += 8 * g->wpr;  // bitmap row
   const int64_t cap = (g->kind == S_BITSET || g->kind == S_BITSET_BB) ? 216 * 1024 : 96 * 1024;
-  return (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, R * row_bytes));
+  const int64_t head = g->kind == S_BB ? 16LL * R : 0;  // CSR+BB: compact row descriptors
+  return (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, head + R * row_bytes));
 }
 
 namespace {
