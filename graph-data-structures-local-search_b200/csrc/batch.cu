@@ -45,7 +45,7 @@ struct BatchJobDev {
   int32_t tenure_policy, tenure, maxt, piter, num_pert, c2_fixed;
   int32_t n_row_blocks, n_chunks, chunk_cols, stage_bytes;
   int32_t orig;             // index in the caller's job array
-  int32_t pad;
+  int32_t adj_mask;         // CSR: adjacent pairs masked out of the w-free sweep
   const int32_t* init;      // MDP: m ids; MaxBS: part[n]
   const long long* draws;   // MaxBS perturbation events x num_pert
   long long draw_events;
@@ -76,6 +76,7 @@ __device__ DevSolver<KeyT> slot_solver(const BatchJobDev& J, const SlotPool<KeyT
   s.c2_fixed = J.c2_fixed;
   s.n_row_blocks = J.n_row_blocks; s.n_chunks = J.n_chunks; s.chunk_cols = J.chunk_cols;
   s.stage_bytes = J.stage_bytes;
+  s.adj_mask = J.adj_mask;
   s.P = (long long)s.m * s.delta;
   s.sol_in = P.sol_in + slot * P.s_m;
   s.sol_out = P.sol_out + slot * P.s_ldc;
@@ -248,7 +249,8 @@ ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_b
     J.n_row_blocks = (H.m + R - 1) / R;
     // tiles as in the plain solver, full row width where it fits; a cluster
     // gets at least one tile per CTA
-    const bool mdp_csr = ST == S_CSR && PROB == P_MDP;
+    const bool mdp_csr = ST == S_CSR && (PROB == P_MDP || H.g->neg_w);
+    J.adj_mask = mdp_csr ? 1 : 0;
     const long long full = ((delta + pc - 1) / pc) * (long long)pc;
     long long max_cols = full;
     if (ST == S_WSWAP) max_cols = 8LL * pc;

@@ -218,7 +218,8 @@ ts_status build_packed(Req& r, int32_t kind) {
   for (int i = 0; i < 4; i++) s.c2_tab[i] = (int32_t)round(0.7 * c1s[i]);
   s.c2_fixed = (int32_t)round(0.7 * r.p.tenure);
   s.n_row_blocks = (m + R - 1) / R;
-  const bool mdp_csr = kind == S_CSR && r.p.problem == P_MDP;
+  const bool mdp_csr = kind == S_CSR && (r.p.problem == P_MDP || r.g->neg_w);
+  s.adj_mask = mdp_csr ? 1 : 0;
   long long cols = ((delta + pc - 1) / pc) * (long long)pc;
   if (kind == S_WSWAP) cols = std::min<long long>(cols, 8LL * pc);
   if (mdp_csr) cols = std::min<long long>(cols, 16LL * pc);
@@ -448,7 +449,7 @@ void ts_server::round() {
         J->need_init = r.started ? 0 : 1;
         J->out = r.d_res;
         J->best_out = r.d_best;
-        const bool mdp_csr = r.kind == S_CSR && r.p.problem == P_MDP;
+        const bool mdp_csr = r.kind == S_CSR && J->s.adj_mask;
         size_t need = 16;
         if (mdp_csr) need = 4 * (size_t)J->s.chunk_cols;
         if (J->s.stage_bytes) need = (size_t)J->s.stage_bytes;

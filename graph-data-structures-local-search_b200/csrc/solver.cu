@@ -290,6 +290,7 @@ struct ts_solver {
   int64_t P = 0;
   int R = 0;
   int32_t n_row_blocks = 0, n_chunks = 0, chunk_cols = 0, stage_bytes = 0;
+  int32_t adj_mask = 0;
   size_t dyn_smem = 0;
   int grid = 0;
   int32_t num_pert = 1;
@@ -320,6 +321,7 @@ struct ts_solver {
     s.c2_fixed = (int32_t)round(0.7 * p.tenure);
     s.n_row_blocks = n_row_blocks; s.n_chunks = n_chunks; s.chunk_cols = chunk_cols;
     s.stage_bytes = stage_bytes;
+    s.adj_mask = adj_mask;
     s.P = P;
     s.sol_in = sol_in.as<int32_t>(); s.sol_out = sol_out.as<int32_t>();
     s.vg_in = vg_in.as<KeyT>(); s.vg_out = vg_out.as<KeyT>();
@@ -535,9 +537,11 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   s->n_row_blocks = (m + s->R - 1) / s->R;
   // Tile geometry.  Staged structures (BB/Hash/Bitset) and MaxBS CSR span the
   // whole row width once there are enough row blocks, so each CTA stages or
-  // joins its rows once per iteration; MDP CSR keeps a per-column mask in
-  // shared memory (<= 16384 columns); WSwap has no per-CTA setup.
-  const bool mdp_csr = g->kind == S_CSR && p->problem == TS_PROBLEM_MDP;
+  // joins its rows once per iteration; masked CSR (MDP, or MaxBS with a
+  // negative weight) keeps a per-column mask in shared memory (<= 16384
+  // columns); WSwap has no per-CTA setup.
+  const bool mdp_csr = g->kind == S_CSR && (p->problem == TS_PROBLEM_MDP || g->neg_w);
+  s->adj_mask = mdp_csr ? 1 : 0;
   const int64_t pc = pass_cols_of(g->kind);  // columns one pass of the CTA covers
   const int64_t full = ((s->delta + pc - 1) / pc) * pc;
   int64_t max_cols = full;
@@ -554,7 +558,10 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   cols = std::max<int64_t>(pc, std::min<int64_t>(cols, max_cols));
   if (g->kind == S_WSWAP) {
     int sms = 0;
-    TS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess) {
+      cudaGetLastError();
+      sms = 0;  // no wave split: the default chunking stands
+    }
     const int64_t slots = (int64_t)wswap_blocks_per_sm(p->problem, s->wide) * sms;
     cols = wave_cols(s->delta, s->n_row_blocks, pc, 8 * pc, 64 * pc, slots, cols);
   }

@@ -597,8 +597,11 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
     // ---------------- fast pass
     uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw);  // CSR + MDP: adjacency per column
     uint4* s_lite = reinterpret_cast<uint4*>(smem_raw);       // CSR+BB: row descriptors
+    // CSR: adjacent pairs leave the w-free sweep (MDP always; MaxBS when a
+    // weight is negative) and are evaluated exactly by the join below
+    const bool masked = PROB == P_MDP || s.adj_mask != 0;
     if (ST == S_CSR) {
-      if (PROB == P_MDP)
+      if (masked)
         for (int32_t c = tid; c < s.chunk_cols; c += blockDim.x) s_mask[c] = 0u;
       if (tid < 32) {
         // row segments and their prefix (one lane per row)
@@ -706,7 +709,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
       // current position of entry k's neighbour, so adjacent pairs of the tile
       // are found with contiguous reads.  They are evaluated exactly here; for
       // MDP they are also masked out of the sweep (their w-free gain would be
-      // an over-estimate; for MaxBS it is an under-estimate and harmless).
+      // an over-estimate).  For MaxBS with every weight >= 0 the w-free gain
+      // is an under-estimate and harmless; a graph with a negative weight
+      // masks them too.
       const int32_t total = s_off[nr];
       for (int32_t f = tid; f < total; f += blockDim.x) {
         int32_t lo = 0, hi = nr - 1;  // row r with s_off[r] <= f < s_off[r+1]
@@ -720,7 +725,7 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         if (c < c0 || c >= c_end) continue;
         const int2 e = g.adj[k];
         if (k > s_rstart[r] && g.adj[k - 1].x == e.x) continue;  // duplicate pair: first entry wins
-        if (PROB == P_MDP) atomicOr(&s_mask[c - c0], 1u << r);
+        if (masked) atomicOr(&s_mask[c - c0], 1u << r);
         const KeyT x = pair_gain<PROB, KeyT>(s_rv[r], ld_st<PERSIST>(s.vg_out + c), e.y);
         if (allowed(s_rtab[r] != 0, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D))
           atomicMax(&s_rowbest[r], x);
@@ -836,7 +841,7 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         uint32_t mk[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          mk[q] = valid[q] ? (PROB == P_MDP ? s_mask[cb + q - c0] : 0u) : 0xffffffffu;
+          mk[q] = valid[q] ? (masked ? s_mask[cb + q - c0] : 0u) : 0xffffffffu;
           if (valid[q] && ct[q]) {
             // Tabu column: a pair is allowed only when aspirated (gain > best - cur).
 #pragma unroll
@@ -960,9 +965,10 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
             if (c >= c_end) break;
             int32_t w = 0;
             if (ST == S_CSR) {
-              // adjacent pairs are matched below from the row's entries; for
-              // MaxBS an adjacent pair's w-free gain never equals the row maximum.
-              if (PROB == P_MDP && ((s_mask[c - c0] >> r) & 1u)) continue;
+              // adjacent pairs are matched below from the row's entries; when
+              // not masked (MaxBS, w >= 0) an adjacent pair's w-free gain never
+              // exceeds its exact gain, so it cannot equal the row maximum alone.
+              if (masked && ((s_mask[c - c0] >> r) & 1u)) continue;
             } else if (ST == S_WSWAP) {
               w = ld_w1<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + c);
             } else {

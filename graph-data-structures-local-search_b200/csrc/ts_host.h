@@ -64,6 +64,7 @@ struct ts_graph {
   int64_t num_edges = 0;
   int64_t entries = 0;
   int64_t max_wdeg = 0;
+  bool neg_w = false;  // some edge weight is negative
   int64_t wpr = 0;
   int64_t hash_slots = 0;
   tsb::DevBuf rowptr, adj, bits, hoff, hkey, hval, rev;

@@ -89,6 +89,11 @@ struct DevSolver {
   int32_t c2_tab[4];      // C2 for C1 = 15, 30, 60, 120 (reference schedule)
   int32_t c2_fixed;
   int32_t n_row_blocks, n_chunks, chunk_cols, stage_bytes;
+  // CSR: adjacent pairs are left out of the w-free sweep (a per-column mask
+  // in shared memory) and evaluated exactly by the join.  Always for MDP; for
+  // MaxBS only when a weight is negative (with w >= 0 the w-free gain of an
+  // adjacent pair under-estimates it and cannot win).
+  int32_t adj_mask;
   int64_t P;
   int32_t* sol_in;
   int32_t* sol_out;

@@ -232,6 +232,24 @@ def test_batch_rejects_bad_jobs(gpu):
     g.close()
 
 
+@pytest.mark.parametrize("kind", ["csr", "csr-bb", "wswap"])
+def test_batch_negative_weights(gpu, kind):
+    """Weights of both signs: the CSR sweep masks adjacent pairs (no w >= 0
+    assumption) in every cluster size."""
+    u, v, w = rand_graph(700, 0.02, 93, wlo=-1000, whi=1000)
+    g = graph(700, u, v, w, kind, T.PROBLEM_MAXBS)
+    gm = graph(700, u, v, w, kind, T.PROBLEM_MDP)
+    specs = []
+    for cl in (1, 2, 4):
+        specs.append(T.BatchJobSpec(g, T.PROBLEM_MAXBS, max_iter=300, tenure_policy=T.TENURE_FIXED,
+                                    tenure=20, piter=60, gamma=24, seed=cl, cluster=cl))
+        specs.append(T.BatchJobSpec(gm, T.PROBLEM_MDP, m=70, max_iter=300, tenure_policy=T.TENURE_FIXED,
+                                    tenure=10, seed=10 + cl, cluster=cl))
+    res = T.batch_solve(specs)
+    for q, (r, sp) in enumerate(zip(res, specs)):
+        assert_same(r, plain(sp), f"job {q}")
+
+
 _SHARED_KERNEL_CHILD = r"""
 import sys
 import numpy as np

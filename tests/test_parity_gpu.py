@@ -171,6 +171,25 @@ def test_maxbs_explicit_partition(gpu, kind):
                 tenure=10, piter=50, gamma=40, seed=12, initial=part)
 
 
+@pytest.mark.parametrize("kind", STRUCTS)
+@pytest.mark.parametrize("n,p", [(120, 0.2), (2600, 0.01)])
+def test_maxbs_negative_weights(gpu, kind, n, p):
+    # Weights of both signs (the instance readers accept negative fixed-point
+    # weights): no sweep may assume w >= 0 for adjacent pairs.  n = 2600 puts
+    # several 1024-column passes in a row.
+    u, v, w = rand_graph(n, p, 41 + n, wlo=-1000, whi=1000)
+    compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=200, tenure_policy=T.TENURE_FIXED,
+                tenure=15, piter=40, gamma=20, seed=5)
+
+
+@pytest.mark.parametrize("kind", STRUCTS)
+def test_mdp_negative_weights(gpu, kind):
+    n, m = 300, 40
+    u, v, w = rand_graph(n, 0.1, 77, wlo=-500, whi=500)
+    compare_run(T.PROBLEM_MDP, kind, n, u, v, w, m=m, iters=300, tenure_policy=T.TENURE_FIXED,
+                tenure=10, seed=4)
+
+
 def test_lookup_interface_all_structures(gpu):
     n = 3000
     u, v, w = rand_graph(n, 0.002, 41, dup=True)

@@ -52,6 +52,10 @@ def requests():
     u, v, w = node_weight_graph(6000, 8.0, 78)
     out.append((6000, u, v, w, T.PROBLEM_MDP, "csr-bb",
                 dict(m=600, max_iter=200, tenure_policy=T.TENURE_REF, tenure=15, seed=6)))
+    # weights of both signs on the masked CSR path (packed)
+    u, v, w = rand_graph(400, 0.03, 91, wlo=-1000, whi=1000)
+    out.append((400, u, v, w, T.PROBLEM_MAXBS, "csr",
+                dict(max_iter=250, tenure_policy=T.TENURE_FIXED, tenure=12, seed=9, piter=50, gamma=16)))
     # explicit starts
     n = 300
     u, v, w = rand_graph(n, 0.05, 90)
