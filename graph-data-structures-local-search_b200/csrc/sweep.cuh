@@ -786,12 +786,28 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
 #pragma unroll
     for (int r = 0; r < R; r++) best[r] = Lim::none;
 
+    // Bitmap structures with every row's bitmap staged: the rows' shared
+    // offsets stay in registers and each pair is one 32-bit shared load and a
+    // bit extract (lean path below).
+    uint32_t rbase[R];
+    bool bm_staged = false;
+    if (ST == S_BITSET || ST == S_BITSET_BB) {
+      bm_staged = true;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const uint64_t* b = s_desc[r].bits;
+        const bool in_smem = r < nr && __isShared(b);
+        bm_staged &= r >= nr || in_smem;
+        rbase[r] = in_smem ? (uint32_t)(reinterpret_cast<const unsigned char*>(b) - smem_raw) : 0u;
+      }
+    }
+
     const int passes = s.chunk_cols / (TPB * kColsPerLane);
     for (int pass = 0; pass < passes; pass++) {
       const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
       const bool lane_on = cb < c_end;
-      if (ST == S_BITSET) {
-        // the hit path cooperates across the warp: leave the loop together
+      if (ST == S_BITSET || ST == S_BITSET_BB) {
+        // the bitmap paths vote across the warp: leave the loop together
         if (__all_sync(0xffffffffu, !lane_on)) break;
       } else if (!lane_on) {
         break;
@@ -873,6 +889,70 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
       } else {
         int32_t vx[4] = {0, 0, 0, 0};
         if (lane_on) load4<PERSIST>(s.sol_out + cb, vx);
+        if ((ST == S_BITSET || ST == S_BITSET_BB) && bm_staged) {
+          // Lean bitmap path.  Columns past the chunk read word 0 of the row
+          // and are masked by `valid`.  Pairs that hit
+          // (rare: deg / n) get their weight from the row in a warp-uniform
+          // branch; when every lane's four columns are valid and non-tabu the
+          // gain goes straight into the maximum.
+          uint32_t wofs[4], bsh[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const uint32_t vv = valid[q] ? (uint32_t)vx[q] : 0u;  // in-bounds word for any lane
+            wofs[q] = (vv >> 5) << 2;
+            bsh[q] = vv & 31u;
+          }
+          const bool simple = valid[0] && valid[1] && valid[2] && valid[3] && !(ct[0] || ct[1] || ct[2] || ct[3]);
+          const bool wsimple = __all_sync(0xffffffffu, simple);
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            if (r >= nr) continue;
+            const KeyT t = s_rv[r];
+            const unsigned char* rb = smem_raw + rbase[r];
+            bool hq[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              hq[q] = valid[q] && ((*reinterpret_cast<const uint32_t*>(rb + wofs[q]) >> bsh[q]) & 1u);
+            int32_t wq[4] = {0, 0, 0, 0};
+            unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
+            if (any) {
+              const RowDesc d = s_desc[r];
+              if (ST == S_BITSET) {
+                // each hit resolved by the whole warp scanning the row 32 entries at a time
+                while (any) {
+                  const int L = __ffs(any) - 1;
+                  any &= any - 1;
+#pragma unroll
+                  for (int q = 0; q < 4; q++) {
+                    const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
+                    if (hv >= 0) {
+                      const int32_t ww = warp_scan_first(d, hv);
+                      if (lane == L) wq[q] = ww;
+                    }
+                  }
+                }
+              } else {
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                  if (hq[q]) wq[q] = bb_lower(d, vx[q]);
+              }
+            }
+            if (wsimple) {
+#pragma unroll
+              for (int q = 0; q < 4; q++) {
+                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
+                best[r] = x > best[r] ? x : best[r];
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < 4; q++) {
+                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
+                if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+              }
+            }
+          }
+          continue;
+        }
 #pragma unroll
         for (int r = 0; r < R; r++) {
           if (r >= nr) continue;
