@@ -585,6 +585,10 @@ def run_served(args):
                                               "p99": pct(plain_lat, 99), "max": float(plain_lat.max())},
                                 "service_s_total": float(sum(service))},
         "identical_to_alone": bool(identical),
+        "slowest": [{"n": reqs[q]["n"], "problem": reqs[q]["problem"], "iters": reqs[q]["iters"],
+                     "executor": got[tickets[q]].executor, "arrival_s": round(arrivals[q], 3),
+                     "latency_s": round(float(lat[q]), 3), "alone_s": round(service[q], 3)}
+                    for q in np.argsort(-lat)[:6]],
         "generation_s": t_gen,
         "clocks": clocks.summary(),
     }

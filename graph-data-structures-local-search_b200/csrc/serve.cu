@@ -142,6 +142,14 @@ struct Req {
   int32_t* d_best = nullptr;
   long long granted = 0;           // packed: iterations granted so far
   bool started = false;
+  // plain: streams per priority level (created on first use), the current
+  // level and the event that orders a move between them
+  cudaStream_t pstream[8] = {};
+  int level = -1;
+  cudaEvent_t moved = nullptr;
+  double spi = 0;      // plain: measured seconds per iteration inside rounds (0: not yet)
+  int64_t last_k = 0;  // plain: iterations enqueued in the last round
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // plain: bracket the last round's launches
 };
 
 int64_t estimate_footprint(const Req& r) {
@@ -167,6 +175,8 @@ using namespace tsb;
 struct ts_server {
   int32_t device = 0;
   int sms = 148;
+  int prio_least = 0, prio_greatest = 0;  // stream priority range (greatest = numerically lowest)
+  double last_round_s = 0;                // wall time of the previous round
   ts_server_opts opts{};
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   std::mutex mu;
@@ -356,6 +366,15 @@ void ts_server::finish(Req& r, ts_status status, const ts_result* res) {
   r.mem.reset();
   if (r.stream) cudaStreamDestroy(r.stream);
   r.stream = nullptr;
+  for (cudaStream_t& ps : r.pstream) {
+    if (ps) cudaStreamDestroy(ps);
+    ps = nullptr;
+  }
+  if (r.moved) cudaEventDestroy(r.moved);
+  r.moved = nullptr;
+  if (r.ev_a) cudaEventDestroy(r.ev_a);
+  if (r.ev_b) cudaEventDestroy(r.ev_b);
+  r.ev_a = r.ev_b = nullptr;
   std::lock_guard<std::mutex> lk(mu);
   stats.completed++;
   stats.active--;
@@ -392,16 +411,49 @@ void ts_server::admit() {
 
 void ts_server::round() {
   const double round_s = opts.round_ms * 1e-3;
-  // plain solves: admit the next iterations and enqueue their launches
+  const double t_round = now_s(t0);
+  // Plain solves get the iterations that fill the round at their measured
+  // speed (the last round's length, at least round_ms, at most 50 ms), so a
+  // large solve never idles while the round waits for the others.
+  const double target_s = std::max(round_s, std::min(last_round_s, 0.05));
+  // plain solves: admit the next iterations and enqueue their launches.
+  // Every solve progresses, on a stream whose priority follows its age (the
+  // oldest highest): the block scheduler starts the older solves' CTAs first
+  // and the younger ones fill the SMs left idle, so a large early arrival is
+  // not slowed to 1/N speed by everything admitted after it.  A solve that
+  // changes rank moves to the stream of its new level, ordered after its
+  // previous stream by an event.
   std::vector<Req*> plain_done;
+  const int levels = std::max(1, prio_least - prio_greatest + 1);
+  int rank = 0;
   for (auto& rp : active) {
     Req& r = *rp;
     if (!r.plain) continue;
-    const double est = 12e-6 + (double)r.P / 1.5e12;
-    const int64_t k = std::max<int64_t>(4, std::min<int64_t>(1 << 16, (int64_t)(round_s / est)));
+    const int level = std::min(rank++, levels - 1);
+    if (level != r.level && r.g) {
+      if (!r.pstream[level])
+        cudaStreamCreateWithPriority(&r.pstream[level], cudaStreamNonBlocking, prio_greatest + level);
+      if (!r.moved) cudaEventCreateWithFlags(&r.moved, cudaEventDisableTiming);
+      if (r.pstream[level] && r.moved && cudaEventRecord(r.moved, r.g->stream) == cudaSuccess &&
+          cudaStreamWaitEvent(r.pstream[level], r.moved, 0) == cudaSuccess) {
+        r.g->stream = r.pstream[level];
+        r.level = level;
+      }
+      cudaGetLastError();
+    }
+    const double est = r.spi > 0 ? r.spi : 12e-6 + (double)r.P / 1.5e12;
+    const int64_t k = std::max<int64_t>(4, std::min<int64_t>(1 << 16, (int64_t)(target_s / est)));
     int64_t adm = 0;
     ts_status rc = ts_solver_prepare(r.solver, k, &adm);
-    if (rc == TS_OK && adm > 0) rc = ts_solver_enqueue(r.solver, adm);
+    r.last_k = 0;
+    if (rc == TS_OK && adm > 0) {
+      if (!r.ev_a) cudaEventCreate(&r.ev_a);
+      if (!r.ev_b) cudaEventCreate(&r.ev_b);
+      const bool timed = r.ev_a && r.ev_b && cudaEventRecord(r.ev_a, r.g->stream) == cudaSuccess;
+      rc = ts_solver_enqueue(r.solver, adm);
+      if (rc == TS_OK && timed && cudaEventRecord(r.ev_b, r.g->stream) == cudaSuccess) r.last_k = adm;
+      cudaGetLastError();
+    }
     if (rc != TS_OK) {
       r.started = false;
       finish(r, rc, nullptr);
@@ -423,7 +475,8 @@ void ts_server::round() {
     std::vector<Req*>& js = kv.second;
     const bool wide = std::get<2>(kv.first) != 0;
     const size_t rec = wide ? sizeof(ServeJobDev<long long>) : sizeof(ServeJobDev<int32_t>);
-    if (!G.stream) cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking);
+    // packed groups hold the small requests: top priority
+    if (!G.stream) cudaStreamCreateWithPriority(&G.stream, cudaStreamNonBlocking, prio_greatest);
     if (G.cap < js.size()) {
       G.cap = std::max<size_t>(64, js.size() * 2);
       if (G.host) cudaFreeHost(G.host);
@@ -490,6 +543,18 @@ void ts_server::round() {
     }
   }
   for (cudaStream_t s : used) cudaStreamSynchronize(s);
+  last_round_s = now_s(t0) - t_round;
+  for (auto& rp : active) {  // speed of each plain solve in this round (shared GPU included)
+    Req& r = *rp;
+    if (!r.plain || r.ticket < 0 || r.last_k <= 0) continue;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, r.ev_a, r.ev_b) != cudaSuccess || ms <= 0) {
+      cudaGetLastError();
+      continue;
+    }
+    const double x = 1e-3 * ms / (double)r.last_k;
+    r.spi = r.spi > 0 ? 0.5 * (r.spi + x) : x;
+  }
   // packed completions
   for (auto& kv : by_group) {
     for (Req* rp : kv.second) {
@@ -561,6 +626,8 @@ ts_status ts_server_create(const ts_server_opts* opts, ts_server** out) {
   if (s->opts.round_ms <= 0) s->opts.round_ms = 5.0;
   if (s->opts.plain_min_pairs <= 0) s->opts.plain_min_pairs = 1LL << 20;
   TS_CUDA(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, dev));
+  TS_CUDA(cudaDeviceGetStreamPriorityRange(&s->prio_least, &s->prio_greatest));
+  if (s->prio_least - s->prio_greatest + 1 > 8) s->prio_least = s->prio_greatest + 7;  // levels kept per request
   int64_t budget = s->opts.max_bytes;
   if (budget <= 0) {
     size_t fr = 0, tot = 0;
