@@ -301,7 +301,7 @@ typedef struct ts_request {
 
 typedef struct ts_server_opts {
   int64_t max_bytes;         /* HBM budget for admitted requests; 0: 60% of free memory */
-  double round_ms;           /* target duration of one round; 0: 5 ms */
+  double round_ms;           /* shortest round (rounds stretch to the last one's length, up to 50 ms); 0: 5 ms */
   int64_t plain_min_pairs;   /* pairs per iteration from which a solve runs plain; 0: 2^20 */
   int32_t reserved[8];
 } ts_server_opts;
