@@ -222,6 +222,20 @@ def run_reference(args):
     return 0
 
 
+def whole_job_value(local_ms: float, ws: int, pairs_per_rank: int, device):
+    """Replicas: every rank evaluates the same number of pairs on its own GPU.
+    The job's time is the slowest rank's device time (all-reduce MAX, the
+    same collective on every rank) and its value all ranks' pairs over it.
+    Returns (max_ms, pairs/s)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max_ms = float(t.item())
+    return t_max_ms, ws * pairs_per_rank / (t_max_ms / 1e3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -309,11 +323,7 @@ def run_ours(args):
         avg_s = ms / 1e3 / args.steps
         per[k] = {"iters_per_s": 1.0 / avg_s, "swap_gains_per_s": P / avg_s, "ms_per_iter": ms / args.steps,
                   "bytes_per_iter": bytes_per_iter[k], "achieved_gbs": bytes_per_iter[k] / avg_s / 1e9}
-    t_local = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-    t_max_ms = float(t_local.item())
-    value = ws * P * len(kinds) * args.steps / (t_max_ms / 1e3)
+    t_max_ms, value = whole_job_value(tot_ms, ws, P * len(kinds) * args.steps, dev)
 
     peak, peak_src = measured_peaks()
     dom = max(kinds, key=lambda k: per[k]["ms_per_iter"])
