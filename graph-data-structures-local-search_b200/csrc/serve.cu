@@ -215,7 +215,7 @@ namespace {
 template <class KeyT>
 ts_status build_packed(Req& r, int32_t kind) {
   const int32_t n = r.n, m = r.m, delta = n - m;
-  const int R = tpb_of(kind) == 512 ? 8 : (kind == S_CSR ? 32 : 16);
+  const int R = rows_of(kind);
   const int pc = pass_cols_of(kind);
   const int64_t ldc = (delta + 3) & ~3;
   DevSolver<KeyT> s;

@@ -268,14 +268,7 @@ int64_t wave_cols(int64_t delta, int64_t rows, int64_t pc, int64_t lo, int64_t c
   return pick;
 }
 
-int rows_per_tile(int kind) {
-  switch (kind) {
-    case S_CSR: return Rows<S_CSR>::R;
-    case S_BITSET: return Rows<S_BITSET>::R;
-    case S_BITSET_BB: return Rows<S_BITSET_BB>::R;
-    default: return Rows<S_HASH>::R;
-  }
-}
+int rows_per_tile(int kind) { return rows_of(kind); }
 
 }  // namespace
 }  // namespace tsb

@@ -44,6 +44,21 @@ template <int ST> struct Rows { static constexpr int R = 16; };
 template <> struct Rows<S_CSR> { static constexpr int R = 32; };
 template <> struct Rows<S_BITSET> { static constexpr int R = 8; };
 template <> struct Rows<S_BITSET_BB> { static constexpr int R = 8; };
+// Hash and CSR+BB: 8 rows per tile.  Hash keeps a tile's staged tables at
+// ~32 KB, so four CTAs share an SM (16 rows: three; 1.3x on the MaxBS conflict
+// graph n = 100,000, 1.16x on the MDP power-law graph n = 200,000); CSR+BB
+// drops to 60 registers and gains 1.1x on both.
+template <> struct Rows<S_HASH> { static constexpr int R = 8; };
+template <> struct Rows<S_BB> { static constexpr int R = 8; };
+// Rows per tile by structure id (host side of the traits above).
+__host__ __device__ inline int rows_of(int st) {
+  return st == S_CSR ? Rows<S_CSR>::R
+       : st == S_BITSET ? Rows<S_BITSET>::R
+       : st == S_BITSET_BB ? Rows<S_BITSET_BB>::R
+       : st == S_HASH ? Rows<S_HASH>::R
+       : st == S_BB ? Rows<S_BB>::R
+       : Rows<S_WSWAP>::R;
+}
 
 template <class KeyT> struct KeyLim;
 template <> struct KeyLim<int32_t> {
