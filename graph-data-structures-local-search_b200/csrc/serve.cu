@@ -477,11 +477,33 @@ void ts_server::round() {
     const size_t rec = wide ? sizeof(ServeJobDev<long long>) : sizeof(ServeJobDev<int32_t>);
     // packed groups hold the small requests: top priority
     if (!G.stream) cudaStreamCreateWithPriority(&G.stream, cudaStreamNonBlocking, prio_greatest);
+    if (!G.stream) {
+      for (Req* r : js) {
+        finish(*r, cuda_fail(cudaGetLastError(), "serve group stream"), nullptr);
+        r->ticket = -1;
+      }
+      continue;
+    }
     if (G.cap < js.size()) {
-      G.cap = std::max<size_t>(64, js.size() * 2);
+      const size_t cap = std::max<size_t>(64, js.size() * 2);
       if (G.host) cudaFreeHost(G.host);
-      cudaMallocHost(&G.host, rec * G.cap);
-      G.table.alloc(rec * G.cap, "alloc serve table");
+      G.host = nullptr;
+      G.cap = 0;
+      ts_status rc = TS_OK;
+      if (cudaMallocHost(&G.host, rec * cap) != cudaSuccess) {
+        G.host = nullptr;
+        rc = cuda_fail(cudaErrorMemoryAllocation, "serve job table (host)");
+      } else {
+        rc = G.table.alloc(rec * cap, "alloc serve table");
+      }
+      if (rc != TS_OK) {
+        for (Req* r : js) {
+          finish(*r, rc, nullptr);
+          r->ticket = -1;
+        }
+        continue;
+      }
+      G.cap = cap;
     }
     size_t smem = 16;
     for (size_t q = 0; q < js.size(); q++) {
