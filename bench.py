@@ -129,7 +129,7 @@ def build_workload(name: str = "config2", n: int = 0):
 
 
 def algorithmic_bytes(kind: str, n: int, m: int, ldc: int, key_bytes: int, deg_in: np.ndarray,
-                      cap_in: np.ndarray, wpr: int) -> int:
+                      cap_in: np.ndarray, wpr: int, w_bytes: int = 4) -> int:
     """Compulsory HBM bytes of one iteration of `kind`: the row and column
     state every structure reads (contributions, tabu stamps, vertex ids) plus
     what its lookups must touch once -- the inside rows' CSR entries, hash
@@ -145,17 +145,23 @@ def algorithmic_bytes(kind: str, n: int, m: int, ldc: int, key_bytes: int, deg_i
     if kind in ("csr-bitset", "csr-bitset-bb"):
         return base + 4 * delta + 8 * m * wpr
     if kind == "wswap":
-        return base + 4 * m * ldc
+        return base + w_bytes * m * ldc
     raise ValueError(kind)
 
 
-def traffic_from_profiles(kind: str):
+def traffic_from_profiles(workload: str, kind: str, grid: int):
+    """DRAM bytes per launch of this structure's iteration kernel on this
+    workload, from an ncu capture of the same build: an entry records the
+    grid it was captured with, and one captured with another grid (another
+    tile shape) is not this kernel's, so it gives None."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        v = d.get("config2", {}).get(kind)
-        return None if v is None else float(v)
+        v = d.get(workload, {}).get(kind)
+        if not isinstance(v, dict) or int(v.get("grid", -1)) != int(grid):
+            return None
+        return float(v["bytes"])
     except Exception:
         return None
 
@@ -271,6 +277,8 @@ def run_ours(args):
 
     # per-structure compulsory bytes, from the state at the start of the timed region
     gi = graphs[kinds[0]].info()
+    solver_grid = {k: solvers[k].info().grid for k in kinds}
+    w_bytes = max(1, solvers["wswap"].info().w_bytes) if "wswap" in kinds else 4
     words = (n + 63) // 64
     wpr = words + (words & 1)
     with torch.cuda.stream(stream):
@@ -287,7 +295,7 @@ def run_ours(args):
     cap_in = np.array([_hash_cap(int(d)) for d in deg_in], np.int64)
     ldc = (n - m + 3) // 4 * 4
     key_bytes = 4 if 4 * gi.max_weighted_degree < (1 << 30) else 8
-    bytes_per_iter = {k: algorithmic_bytes(k, n, m, ldc, key_bytes, deg_in, cap_in, wpr) for k in kinds}
+    bytes_per_iter = {k: algorithmic_bytes(k, n, m, ldc, key_bytes, deg_in, cap_in, wpr, w_bytes) for k in kinds}
     del rowptr
 
     ev = {k: [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -314,6 +322,12 @@ def run_ours(args):
     for k in kinds:
         it = solvers[k].sync()
         assert it == total, (k, it, total)
+    # every structure ran the same search from the same start: same state
+    ref_state = solvers[kinds[0]].state()
+    for k in kinds[1:]:
+        for a, b in zip(ref_state, solvers[k].state()):
+            assert np.array_equal(a, b), f"{k} ended the timed steps in another state than {kinds[0]}"
+    agree = {"structures_agree": True, "checked": "sol, pos, tabu and contributions after the timed steps"}
     per = {}
     tot_ms = 0.0
     for k in kinds:
@@ -328,7 +342,7 @@ def run_ours(args):
     peak, peak_src = measured_peaks()
     dom = max(kinds, key=lambda k: per[k]["ms_per_iter"])
     achieved = per[dom]["achieved_gbs"]
-    traffic = traffic_from_profiles(dom)
+    traffic = traffic_from_profiles(args.workload, dom, solver_grid[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "kernel": f"iter_kernel[{dom}]",
                 "peak_source": peak_src,
@@ -338,8 +352,16 @@ def run_ours(args):
         roofline["hbm_bound_kernel"] = {"kernel": "iter_kernel[wswap]", "achieved": per["wswap"]["achieved_gbs"],
                                         "frac": per["wswap"]["achieved_gbs"] / peak}
 
+    for k in kinds:
+        solvers[k].close()
+        graphs[k].close()
+    del flush
+    torch.cuda.empty_cache()
+
     line = None
     if rank == 0:
+        configs = None if (args.no_extras or args.no_configs) else run_configs(T, torch, dev, stream, kinds)
+        ref_cuda = None if (args.no_extras or args.no_configs) else run_reference_cuda(configs)
         e2e = None if args.no_extras else run_e2e(T, torch, wl, kinds, args, seed, problem, m)
         cpu = None if args.no_extras else cpu_baseline_sample(wl, problem, m)
         batched = None if (args.no_extras or args.no_batched) else run_batched(T, torch, dev, args)
@@ -356,14 +378,14 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "agreement": agree,
+            "configs": configs,
+            "reference_cuda": ref_cuda,
             "batched": batched,
             "gpu_launches": len(kinds) * args.steps,
             "clocks": clocks.summary(),
             "wall_s_timed_region": wall,
         }
-    for k in kinds:
-        solvers[k].close()
-        graphs[k].close()
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -378,6 +400,179 @@ def _hash_cap(deg: int) -> int:
     while cap < 4 * deg:
         cap <<= 1
     return cap
+
+
+def time_structures(T, torch, dev, stream, wl, problem, m, kinds, iters, warmup, flush_between, seed=1):
+    """Plain solves of one workload, one structure at a time (built, started
+    from the same seeded state, `warmup` untimed iterations, then `iters`
+    timed ones).  flush_between: a 256 MiB buffer is written before every
+    timed iteration (outside its events); otherwise the iterations run back
+    to back between one pair of events, as a caller's loop runs them.
+    Returns per structure it/s, swap-gains/s and the state reached."""
+    n = wl["n"]
+    P = m * (n - m)
+    mdp = problem == T.PROBLEM_MDP
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev) if flush_between else None
+    out = {}
+    for k in kinds:
+        g = T.Graph(n, wl["u"], wl["v"], wl["w"], k, drop_self_loops=mdp, stream=stream.cuda_stream)
+        s = T.Solver(g, problem, m=m if mdp else 0, max_iter=10**9, tenure_policy=T.TENURE_FIXED,
+                     tenure=wl["tenure"], piter=500, gamma=150, seed=seed)
+        try:
+            s.init(None)
+            assert s.prepare(warmup + iters) == warmup + iters
+            with torch.cuda.stream(stream):
+                s.enqueue(warmup)
+            torch.cuda.synchronize(dev)
+            evs = []
+            with torch.cuda.stream(stream):
+                if flush is None:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    s.enqueue(iters)
+                    b.record(stream)
+                    evs.append((a, b))
+                else:
+                    for _ in range(iters):
+                        flush.zero_()
+                        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        a.record(stream)
+                        s.enqueue(1)
+                        b.record(stream)
+                        evs.append((a, b))
+            torch.cuda.synchronize(dev)
+            assert s.sync() == warmup + iters
+            ms = sum(a.elapsed_time(b) for a, b in evs)
+            st = s.state()
+            si = s.info()
+        finally:
+            s.close()
+            g.close()
+        sec = ms / 1e3 / iters
+        out[k] = {"iters_per_s": 1.0 / sec, "swap_gains_per_s": P / sec, "ms_per_iter": ms / iters,
+                  "grid": si.grid, "w_bytes": si.w_bytes, "_state": st}
+    states = [out[k].pop("_state") for k in kinds]
+    same = all(all(np.array_equal(a, b) for a, b in zip(states[0], st)) for st in states[1:])
+    return out, same, states[0]
+
+
+def run_configs(T, torch, dev, stream, kinds):
+    """Config 1 (MDP ER n=2000, m=200, tenure 20) and config 3 (MDP Chung-Lu
+    n=200000, m=2000, tenure 100) per structure, plus config 3's graph at
+    m=1000 (the only m at which the reference's own loaders accept that
+    graph, see run_reference_cuda).  Config 1's iterations run back to back
+    (its whole state is a few hundred KB); config 3's are timed one at a time
+    with L2 flushed between them and reported against the HBM roofline."""
+    from ts_b200 import gen
+    peak, peak_src = measured_peaks()
+    res = {}
+    c1 = gen.config1()
+    per, same, _ = time_structures(T, torch, dev, stream, c1, T.PROBLEM_MDP, c1["m"], kinds, iters=3000,
+                                   warmup=200, flush_between=False)
+    res["config1"] = {"workload": WORKLOADS["config1"][1], "timed": "iterations 201-3200, back to back",
+                      "per_structure": per, "structures_agree": same}
+    c3 = gen.config3()
+    n, m = c3["n"], c3["m"]
+    per, same, st = time_structures(T, torch, dev, stream, c3, T.PROBLEM_MDP, m, kinds, iters=30, warmup=5,
+                                    flush_between=True)
+    deg = np.bincount(np.concatenate([c3["u"], c3["v"]]), minlength=n).astype(np.int64)
+    sol = st[0]
+    deg_in = deg[sol[:m]]
+    cap_in = np.array([_hash_cap(int(d)) for d in deg_in], np.int64)
+    words = (n + 63) // 64
+    wpr = words + (words & 1)
+    ldc = (n - m + 3) // 4 * 4
+    for k in kinds:
+        b = algorithmic_bytes(k, n, m, ldc, 4, deg_in, cap_in, wpr, w_bytes=max(1, per[k]["w_bytes"]))
+        per[k]["bytes_per_iter"] = b
+        per[k]["achieved_gbs"] = b * per[k]["iters_per_s"] / 1e9
+        per[k]["hbm_frac"] = per[k]["achieved_gbs"] / peak
+    res["config3"] = {"workload": WORKLOADS["config3"][1], "timed": "iterations 6-35, 256 MiB L2 flush before each",
+                      "per_structure": per, "structures_agree": same, "peak_gbs": peak, "peak_source": peak_src}
+    c3b = dict(c3, m=1000)
+    per, same, _ = time_structures(T, torch, dev, stream, c3b, T.PROBLEM_MDP, 1000, kinds, iters=30, warmup=5,
+                                   flush_between=True)
+    res["config3_m1000"] = {"workload": "config3 graph with m=1000 (the reference's b2500 loader fixes m=1000)",
+                            "timed": "iterations 6-35, 256 MiB L2 flush before each", "per_structure": per,
+                            "structures_agree": same}
+    return res
+
+
+def _write_instance(path, n, u, v, w, header, one_based):
+    import pandas as pd
+    with open(path, "w") as f:
+        f.write(header + "\n")
+    off = 1 if one_based else 0
+    pd.DataFrame({"a": u.astype(np.int64) + off, "b": v.astype(np.int64) + off, "w": w}).to_csv(
+        path, sep=" ", header=False, index=False, mode="a")
+
+
+REF_MDP_ALGS = ["csr", "csr-bb", "csr-bitset-bb", "hash", "wswap"]
+
+
+def run_reference_cuda(configs):
+    """The reference's own CUDA programs, built unmodified from its sources by
+    oracle/build_ref.sh (linked with a shim that injects the seed, stamps
+    every ArgMax copy with a monotonic clock and exits after a set number of
+    them), timed on this GPU.  Iterations/s = ArgMax copies between the first
+    and the last stamp / elapsed time of the first tabu call.
+      config 1: MDG-a file "2000 200" (the exact config);
+      config 3's graph: the MDG-a header computes n(n-1)/2 in int, which
+        overflows at n = 200,000, and the other loaders fix m (sparse/nenad
+        100, b2500 1000, p3000-5000 n/2 -- too many pairs for int indices),
+        so the b2500 loader runs it, at m = 1000, beside this engine at m = 1000.
+    GPU-MDP-CSR-Bitset.cu does not compile (syntax error); the Hash program
+    packs (u<<16)|v into 32 bits, so its lookups alias above n = 65,536."""
+    import tempfile
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not all(os.path.exists(os.path.join(ref_dir, f"mdp_{a}")) for a in REF_MDP_ALGS):
+        return {"unavailable": "reference programs not built (oracle/_ref); oracle/build_ref.sh builds them"}
+    from ts_b200 import gen
+    out = {"what": "the reference's own CUDA programs, unmodified, on this GPU; iterations/s of their first "
+                   "tabu call (ArgMax copy stamps)",
+           "csr-bitset": "not buildable (GPU-MDP-CSR-Bitset.cu does not compile)"}
+    cases = [("config1", gen.config1(), "MDG-a", 3000, False),
+             ("config3_m1000", gen.config3(), "b2500", 30, True)]
+    with tempfile.TemporaryDirectory() as td:
+        for name, wl, fmt, limit, one_based in cases:
+            n = wl["n"]
+            path = os.path.join(td, name + ".txt")
+            if fmt == "MDG-a":
+                _write_instance(path, n, wl["u"], wl["v"], wl["w"], f"{n} {wl['m']}", False)
+            else:
+                _write_instance(path, n, wl["u"], wl["v"], wl["w"], f"{n} {len(wl['u'])}", True)
+            per = {}
+            for alg in REF_MDP_ALGS:
+                trace = os.path.join(td, f"{name}_{alg}.trace")
+                env = dict(os.environ, TS_REF_TRACE=trace, TS_REF_N=str(n), TS_REF_SEED="1",
+                           TS_REF_LIMIT=str(limit))
+                cmd = f'ulimit -s unlimited; exec "{os.path.join(ref_dir, "mdp_" + alg)}" "{path}" {fmt} 100000 1'
+                t0 = time.time()
+                try:
+                    r = subprocess.run(["bash", "-c", cmd], env=env, stdin=subprocess.DEVNULL,
+                                       stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, timeout=300)
+                    rc = r.returncode
+                except subprocess.TimeoutExpired:
+                    rc = "timeout"
+                wall = time.time() - t0
+                ts = []
+                if os.path.exists(trace):
+                    with open(trace) as f:
+                        ts = [int(x.split()[3]) for x in f if x.startswith("A ")]
+                if rc != 0 or len(ts) < 3:
+                    per[alg] = {"error": f"exit {rc}, {len(ts)} ArgMax records", "wall_s": wall}
+                    continue
+                sec = (ts[-1] - ts[0]) / 1e9
+                d = {"iters_per_s": (len(ts) - 1) / sec, "iterations": len(ts), "wall_s": wall}
+                if alg == "hash" and n > 65536:
+                    d["note"] = "incorrect at this n: (u<<16)|v keys alias above n = 65,536"
+                ours = (configs or {}).get(name, {}).get("per_structure", {}).get(alg)
+                if ours:
+                    d["ours_iters_per_s"] = ours["iters_per_s"]
+                    d["speedup"] = ours["iters_per_s"] / d["iters_per_s"]
+                per[alg] = d
+            out[name] = per
+    return out
 
 
 def run_e2e(T, torch, wl, kinds, args, seed, problem, m):
@@ -618,6 +813,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="config2/config3 at another size (profiling cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, CPU-baseline and batched legs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (config 4) leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the config-1/config-3 legs and the reference CUDA build's timing")
     ap.add_argument("--c4-instances", type=int, default=40, help="batched leg: instances of config 4")
     ap.add_argument("--c4-plain-sample", type=int, default=24, help="batched leg: solves run plain")
     ap.add_argument("--tune-budget", type=float, default=30.0, help="autotuner time budget (s)")

@@ -1,9 +1,8 @@
 // noalloc.cu -- best admissible swap of a caller-held state, with no device
 // allocation.
 //
-// Who needs it: callers that may not allocate device memory -- code recorded
-// inside a CUDA stream capture (cudaMalloc is not permitted there), plugins
-// whose host application owns all of HBM through its own pool allocator, and
+// Who needs it: callers that may not allocate device memory -- plugins whose
+// host application owns all of HBM through its own pool allocator, and
 // services that run under a fixed device-memory budget.  They keep the graph
 // and the tabu state in their own buffers and get one iteration's decision:
 // every swap evaluated with the reference's key rule (tabu/aspiration filter,
@@ -16,6 +15,12 @@
 // exits.  All calls share it and it keeps the last call's contents: the ticket
 // is cleared by the staging kernel of every call, and calls that overlap on the
 // GPU (from other streams or host threads) race on it.
+//
+// Cost: one thread per swap pair, each with its own binary search of the
+// inside vertex's CSR row in global memory -- about log2(degree) + 2 dependent
+// loads per pair, so a call over P pairs takes roughly P / 1e10 seconds on a
+// B200 (n = 262,144 with m = n/2 is ~1.7e10 pairs: seconds per call).  It is
+// meant for modest instances, not as the fast path.
 #include <climits>
 #include <cstdint>
 #include <mutex>
@@ -125,7 +130,32 @@ k_na_sweep(int32_t problem, int32_t n, int32_t m, long long cur, long long best,
 
 constexpr int kMaxDevices = 64;
 std::mutex g_na_mu;
-void* g_na_addr[kMaxDevices];
+// The scratch array has one address per CUDA context: cached per device
+// together with the context it was looked up in, and looked up again when the
+// caller's current context on that device is another one (a context the caller
+// created itself, or a new primary context after a device reset).
+struct NaAddr {
+  void* ctx;
+  void* addr;
+};
+NaAddr g_na_addr[kMaxDevices];
+
+// cuCtxGetCurrent, reached through the runtime so the library needs no
+// link-time dependency on the driver library.
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  return fn;
+}
 
 }  // namespace
 }  // namespace tsb
@@ -156,16 +186,34 @@ extern "C" ts_status ts_best_swap_noalloc(int32_t problem, int32_t n, int32_t m,
   if (dev < 0 || dev >= kMaxDevices) { set_error("ts_best_swap_noalloc: device index out of range"); return TS_ERR_UNSUPPORTED; }
   void* base = nullptr;
   {
-    // Once per device, with that device current: the scratch array's device
-    // address (its name in host code is only a host-side stand-in).
+    // With the caller's device current: the scratch array's device address in
+    // the current context (its name in host code is only a host-side
+    // stand-in).  The first call in a context looks it up; later calls in the
+    // same context reuse it.
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    if (!get_ctx) {
+      set_error("ts_best_swap_noalloc: cuCtxGetCurrent is not available from the driver");
+      return TS_ERR_UNSUPPORTED;
+    }
+    void* ctx = nullptr;
+    if (get_ctx(&ctx) != 0 || !ctx) {
+      // No context bound to this thread yet: bind the device's primary context
+      // (cudaSetDevice initialises it) -- the one the runtime would use.
+      TS_CUDA(cudaSetDevice(dev));
+      if (get_ctx(&ctx) != 0 || !ctx) {
+        set_error("ts_best_swap_noalloc: no current CUDA context on the calling thread");
+        return TS_ERR_CUDA;
+      }
+    }
     std::lock_guard<std::mutex> lock(g_na_mu);
-    if (!g_na_addr[dev]) {
+    if (g_na_addr[dev].ctx != ctx || !g_na_addr[dev].addr) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
       if (e != cudaSuccess) return cuda_fail(e, "ts_best_swap_noalloc: cudaGetSymbolAddress");
-      g_na_addr[dev] = p;
+      g_na_addr[dev].ctx = ctx;
+      g_na_addr[dev].addr = p;
     }
-    base = g_na_addr[dev];
+    base = g_na_addr[dev].addr;
   }
   const NaView sc = view_of(base);
   cudaStream_t st = static_cast<cudaStream_t>(stream);

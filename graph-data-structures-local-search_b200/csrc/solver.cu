@@ -931,6 +931,20 @@ ts_status ts_perturb_draws(int32_t n, uint32_t seed, int32_t gamma, int32_t init
   return TS_OK;
 }
 
+ts_status ts_solver_info_get(const ts_solver* s, ts_solver_info* out) {
+  if (!s || !out) { set_error("ts_solver_info_get: NULL argument"); return TS_ERR_INVALID_ARG; }
+  std::memset(out, 0, sizeof(*out));
+  out->grid = s->grid;
+  out->tile_rows = s->R;
+  out->chunk_cols = s->chunk_cols;
+  out->n_chunks = s->n_chunks;
+  out->threads = tpb_of(s->g->kind);
+  out->dyn_smem_bytes = (int32_t)s->dyn_smem;
+  out->key_bytes = s->wide ? 8 : 4;
+  out->w_bytes = s->g->kind == S_WSWAP ? 4 : 0;
+  return TS_OK;
+}
+
 ts_status ts_solver_destroy(ts_solver* s) {
   if (!s) return TS_OK;
   cudaSetDevice(s->g->device);

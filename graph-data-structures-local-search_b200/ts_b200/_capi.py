@@ -27,7 +27,7 @@ EXPORTS = [
     "ts_graph_create", "ts_graph_create_device", "ts_graph_info_get", "ts_graph_destroy",
     "ts_lookup", "ts_lookup_host", "ts_params_default", "ts_solver_create", "ts_solver_init",
     "ts_solver_step", "ts_solver_result", "ts_solver_state", "ts_solver_trace",
-    "ts_solver_destroy", "ts_random_start", "ts_perturb_draws", "ts_solver_prepare",
+    "ts_solver_destroy", "ts_solver_info_get", "ts_random_start", "ts_perturb_draws", "ts_solver_prepare",
     "ts_solver_enqueue", "ts_solver_sync", "ts_best_swap_noalloc",
     "ts_batch_create", "ts_batch_launch", "ts_batch_sync", "ts_batch_results", "ts_batch_info_get",
     "ts_batch_destroy", "ts_batch_run", "ts_solver_set_perturbations",
@@ -48,6 +48,14 @@ class GraphInfo(ctypes.Structure):
         ("num_entries", ctypes.c_int64), ("max_weighted_degree", ctypes.c_int64),
         ("device_bytes", ctypes.c_int64), ("hash_slots", ctypes.c_int64),
         ("bitset_words_per_row", ctypes.c_int64),
+    ]
+
+
+class SolverInfo(ctypes.Structure):
+    _fields_ = [
+        ("grid", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("chunk_cols", ctypes.c_int32),
+        ("n_chunks", ctypes.c_int32), ("threads", ctypes.c_int32), ("dyn_smem_bytes", ctypes.c_int32),
+        ("key_bytes", ctypes.c_int32), ("w_bytes", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
     ]
 
 
@@ -176,6 +184,8 @@ def lib():
     L.ts_solver_trace.argtypes = [P, P, I64, ctypes.POINTER(I64)]
     L.ts_solver_destroy.restype = st
     L.ts_solver_destroy.argtypes = [P]
+    L.ts_solver_info_get.restype = st
+    L.ts_solver_info_get.argtypes = [P, ctypes.POINTER(SolverInfo)]
     L.ts_solver_prepare.restype = st
     L.ts_solver_prepare.argtypes = [P, I64, ctypes.POINTER(I64)]
     L.ts_solver_enqueue.restype = st

@@ -189,6 +189,12 @@ class Solver:
                 "ts_solver_state")
         return sol, pos, tab, vg
 
+    def info(self) -> C.SolverInfo:
+        """Launch geometry and element widths of the iteration kernel."""
+        out = C.SolverInfo()
+        C.check(C.lib().ts_solver_info_get(self._h, ctypes.byref(out)), "ts_solver_info_get")
+        return out
+
     def trace(self) -> np.ndarray:
         cnt = ctypes.c_int64(0)
         C.check(C.lib().ts_solver_trace(self._h, None, 0, ctypes.byref(cnt)), "ts_solver_trace")

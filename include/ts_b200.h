@@ -79,6 +79,20 @@ typedef struct ts_graph_info {
   int64_t bitset_words_per_row;
 } ts_graph_info;
 
+/* Launch geometry of a solver's iteration kernel (no counterpart in the
+ * reference, whose kernels use one thread per pair): ts_solver_info. */
+typedef struct ts_solver_info {
+  int32_t grid;           /* CTAs per iteration launch (one tile each) */
+  int32_t tile_rows;      /* inside positions per tile */
+  int32_t chunk_cols;     /* outside positions per tile */
+  int32_t n_chunks;       /* tiles per row block */
+  int32_t threads;        /* threads per CTA */
+  int32_t dyn_smem_bytes; /* dynamic shared memory per CTA */
+  int32_t key_bytes;      /* 4: 32-bit pair keys and contributions, 8: 64-bit */
+  int32_t w_bytes;        /* WSwap: bytes per matrix element (2 or 4); 0 otherwise */
+  int32_t reserved[8];
+} ts_solver_info;
+
 typedef struct ts_params {
   int32_t problem;        /* ts_problem */
   int32_t m;              /* MDP: selected-set size; MaxBS: ignored (floor(n/2), GPU-MAXBS-CSR.cu:151) */
@@ -202,6 +216,8 @@ ts_status ts_solver_result(ts_solver* s, ts_result* out, int32_t* best_sol);
 ts_status ts_solver_state(ts_solver* s, int32_t* sol, int32_t* pos, int32_t* tab, int64_t* vg);
 /* Copies up to cap trace records (params.trace=1). */
 ts_status ts_solver_trace(ts_solver* s, ts_trace_rec* out, int64_t cap, int64_t* n_out);
+/* Launch geometry and element widths the solver picked (ts_solver_info). */
+ts_status ts_solver_info_get(const ts_solver* s, ts_solver_info* out);
 ts_status ts_solver_destroy(ts_solver* s);
 
 /* ---------------------------------------------------------------- host helpers
@@ -339,13 +355,13 @@ ts_status ts_server_destroy(ts_server* s);
 
 /* ---------------------------------------------------------------- no allocation
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory -- code recorded in a CUDA stream capture (cudaMalloc is not allowed
- * there), plugins whose host application owns all of HBM through its own pool,
- * services held to a fixed device-memory budget.  From a tabu state the caller
- * keeps in its own device buffers, evaluates every swap of one iteration with
- * the reference's key rule and ArgMax tie rule and writes the decision; it
- * allocates nothing, using a fixed scratch array compiled into the library
- * (about 3 MiB, held on every GPU that loads the library until exit).
+ * memory -- plugins whose host application owns all of HBM through its own
+ * pool, services held to a fixed device-memory budget.  From a tabu state the
+ * caller keeps in its own device buffers, evaluates every swap of one
+ * iteration with the reference's key rule and ArgMax tie rule and writes the
+ * decision; it allocates nothing, using a fixed scratch array compiled into
+ * the library (about 3 MiB, held on every GPU that loads the library until
+ * exit).
  *   d_rowptr int64[n+1], d_col / d_w int32[entries]: CSR rows sorted by
  *     neighbour id (the first entry of a duplicated pair is the one used);
  *   d_sol int32[n]: vertex at each position, the inside set at [0, m);
@@ -353,10 +369,12 @@ ts_status ts_server_destroy(ts_server* s);
  *   iter, cur, best: iteration counter and objective bookkeeping;
  *   d_out int64[2]: {key, flat index i*(n-m)+(j-m)} of the chosen swap.
  * n above TS_NOALLOC_MAX_N is rejected (TS_ERR_INVALID_ARG).  Work runs on
- * `stream` without synchronising.  The first call on a device looks the
- * scratch address up and should come before any stream capture.  All calls
- * share the scratch, so calls that overlap on the GPU (other streams or host
- * threads) race on it. */
+ * `stream` without synchronising, in the CUDA context current on the calling
+ * thread (the device's primary context if none is).  The first call in each
+ * context looks the scratch address up; it should come before any stream
+ * capture.  All calls share the scratch, so calls that overlap on the GPU
+ * (other streams or host threads) race on it.  Cost: one binary search of a
+ * global CSR row per pair, roughly P / 1e10 s for P = m*(n-m) pairs. */
 #define TS_NOALLOC_MAX_N 262144
 ts_status ts_best_swap_noalloc(int32_t problem, int32_t n, int32_t m, int64_t iter, int64_t cur,
                                int64_t best, const int64_t* d_rowptr, const int32_t* d_col,

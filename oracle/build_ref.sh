@@ -4,6 +4,9 @@
 # (trace + seed wrappers).  Output: oracle/_ref/{mdp,maxbs}_<alg> (git-ignored).
 # The sources are compiled where they lie; nothing is copied.
 #   usage: oracle/build_ref.sh [reference_dir]
+# The reference directory comes from the argument, else TS_REFERENCE_DIR, else
+# the checkout location of the machine this repository is built on (this
+# script is the one place that names it).
 set -u
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF="${1:-${TS_REFERENCE_DIR:-/root/reference}}"

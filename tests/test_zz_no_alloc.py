@@ -1,9 +1,8 @@
 """ts_best_swap_noalloc: one iteration's decision without any device allocation.
 
-Some callers cannot allocate device memory: code recorded inside a CUDA stream
-capture (cudaMalloc is not allowed there), plugins whose host application owns
-all of the GPU's memory through its own pool, and services held to a fixed
-device-memory budget.  They keep the graph and the tabu state in their own
+Some callers cannot allocate device memory: plugins whose host application
+owns all of the GPU's memory through its own pool, and services held to a
+fixed device-memory budget.  They keep the graph and the tabu state in their own
 buffers and ask the library which swap the next iteration makes; the library
 then works in a fixed scratch array compiled into it.
 
