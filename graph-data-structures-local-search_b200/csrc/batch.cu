@@ -46,6 +46,7 @@ struct BatchJobDev {
   int32_t n_row_blocks, n_chunks, chunk_cols, stage_bytes;
   int32_t orig;             // index in the caller's job array
   int32_t adj_mask;         // CSR: adjacent pairs masked out of the w-free sweep
+  int32_t tile_rows, fast, fast_ecap;  // tile shape (tile_geometry)
   const int32_t* init;      // MDP: m ids; MaxBS: part[n]
   const long long* draws;   // MaxBS perturbation events x num_pert
   long long draw_events;
@@ -77,6 +78,10 @@ __device__ DevSolver<KeyT> slot_solver(const BatchJobDev& J, const SlotPool<KeyT
   s.n_row_blocks = J.n_row_blocks; s.n_chunks = J.n_chunks; s.chunk_cols = J.chunk_cols;
   s.stage_bytes = J.stage_bytes;
   s.adj_mask = J.adj_mask;
+  s.tile_rows = J.tile_rows;
+  s.fast = J.fast;
+  s.fast_ecap = J.fast_ecap;
+  s.w16 = 0;  // slot pools hold 32-bit matrices
   s.P = (long long)s.m * s.delta;
   s.sol_in = P.sol_in + slot * P.s_m;
   s.sol_out = P.sol_out + slot * P.s_ldc;
@@ -246,28 +251,18 @@ ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_b
     BatchJobDev& J = table[G.job_off + q];
     const int32_t delta = H.n - H.m;
     const long long ldc = (delta + 3) & ~3;
-    J.n_row_blocks = (H.m + R - 1) / R;
     // tiles as in the plain solver, full row width where it fits; a cluster
     // gets at least one tile per CTA
-    const bool mdp_csr = ST == S_CSR && (PROB == P_MDP || H.g->neg_w);
-    J.adj_mask = mdp_csr ? 1 : 0;
-    const long long full = ((delta + pc - 1) / pc) * (long long)pc;
-    long long max_cols = full;
-    if (ST == S_WSWAP) max_cols = 8LL * pc;
-    if (mdp_csr) max_cols = 16LL * pc;
-    const long long want_chunks = std::max<long long>(1, (cs + J.n_row_blocks - 1) / J.n_row_blocks);
-    long long cols = (delta + want_chunks - 1) / want_chunks;
-    cols = ((cols + pc - 1) / pc) * pc;
-    cols = std::max<long long>(pc, std::min<long long>(cols, max_cols));
-    J.chunk_cols = (int32_t)cols;
-    J.n_chunks = (int32_t)((delta + cols - 1) / cols);
-    J.stage_bytes = 0;
-    size_t need = 16;
-    if (mdp_csr) need = sizeof(uint32_t) * (size_t)cols;
-    if (ST == S_HASH || ST == S_BB || ST == S_BITSET || ST == S_BITSET_BB) {
-      J.stage_bytes = staging_bytes(H.g, R);
-      need = (size_t)J.stage_bytes;
-    }
+    const TileGeom tg = tile_geometry(H.g, PROB, H.m, sizeof(KeyT) == 8, cs, H.p.pass);
+    J.n_row_blocks = tg.n_row_blocks;
+    J.tile_rows = tg.rows;
+    J.fast = tg.fast;
+    J.fast_ecap = tg.fast_ecap;
+    J.adj_mask = tg.adj_mask;
+    J.chunk_cols = tg.chunk_cols;
+    J.n_chunks = tg.n_chunks;
+    J.stage_bytes = tg.stage_bytes;
+    const size_t need = tg.smem;
     smem = std::max(smem, need);
     max_m = std::max<long long>(max_m, H.m);
     max_n = std::max<long long>(max_n, H.n);

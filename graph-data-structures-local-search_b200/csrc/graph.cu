@@ -99,19 +99,23 @@ __global__ void k_pack_adj(int64_t N, const unsigned long long* __restrict__ key
 }
 
 // Per-row sum |w|: bounds |contribution| and decides the 32-bit key path
-// (out[0]); out[1] != 0 when some weight is negative.
+// (out[0]); out[1] != 0 when some weight is negative; out[2] = max |w| (the
+// WSwap matrix holds 16-bit weights when it fits).
 __global__ void k_max_wdeg(int32_t n, const int64_t* __restrict__ rowptr,
                            const int2* __restrict__ adj, unsigned long long* __restrict__ out) {
   for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    unsigned long long s = 0;
+    unsigned long long s = 0, mx = 0;
     bool neg = false;
     for (int64_t k = rowptr[r]; k < rowptr[r + 1]; k++) {
       int32_t x = adj[k].y;
-      s += (unsigned long long)(x < 0 ? -(long long)x : (long long)x);
+      const unsigned long long a = (unsigned long long)(x < 0 ? -(long long)x : (long long)x);
+      s += a;
+      mx = a > mx ? a : mx;
       neg |= x < 0;
     }
     atomicMax(out, s);
     if (neg) atomicMax(out + 1, 1ull);
+    if (mx) atomicMax(out + 2, mx);
   }
 }
 
@@ -282,7 +286,7 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
   if ((s = vals.alloc(sizeof(int32_t) * N2, "alloc vals")) != TS_OK) return s;
   if ((s = vals_alt.alloc(sizeof(int32_t) * N2, "alloc vals")) != TS_OK) return s;
   if ((s = err.alloc(sizeof(int32_t) * 2, "alloc err")) != TS_OK) return s;
-  if ((s = cnt.alloc(2 * sizeof(unsigned long long), "alloc cnt")) != TS_OK) return s;
+  if ((s = cnt.alloc(3 * sizeof(unsigned long long), "alloc cnt")) != TS_OK) return s;
   TS_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int32_t) * 2, st));
   if (E > 0) {
     k_make_keys<<<blocks_for(E), kTPB, 0, st>>>(n, E, d_u, d_v, d_w, G->drop_self_loops,
@@ -316,7 +320,9 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
   const int64_t N = G->h_rowptr[n];
   G->entries = N;
   G->num_edges = N / 2;
-  if ((s = G->adj.alloc(sizeof(int2) * N, "alloc adj")) != TS_OK) return s;
+  // Two spare entries: the sweep bulk-copies rows from an even entry to an
+  // even end (16-byte aligned), which can reach one entry past the last row.
+  if ((s = G->adj.alloc(sizeof(int2) * (N + 2), "alloc adj")) != TS_OK) return s;
   if (N > 0) {
     k_pack_adj<<<blocks_for(N), kTPB, 0, st>>>(N, dk.Current(), dv.Current(), G->adj.as<int2>());
     TS_CUDA(cudaGetLastError());
@@ -326,13 +332,13 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
   vals.release();
   vals_alt.release();
   tmp.release();
-  TS_CUDA(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(unsigned long long), st));
+  TS_CUDA(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), st));
   if (n > 0) {
     k_max_wdeg<<<blocks_for(n), kTPB, 0, st>>>(n, G->rowptr.as<int64_t>(), G->adj.as<int2>(),
                                                cnt.as<unsigned long long>());
     TS_CUDA(cudaGetLastError());
   }
-  unsigned long long mw[2] = {0, 0};
+  unsigned long long mw[3] = {0, 0, 0};
   TS_CUDA(cudaMemcpyAsync(mw, cnt.p, sizeof(mw), cudaMemcpyDeviceToHost, st));
 
   if (G->kind == TS_STRUCT_CSR_BITSET || G->kind == TS_STRUCT_CSR_BITSET_BB) {
@@ -392,6 +398,7 @@ static ts_status build_graph(ts_graph* G, int64_t E, const int32_t* d_u, const i
   }
   G->max_wdeg = (int64_t)mw[0];
   G->neg_w = mw[1] != 0;
+  G->max_abs_w = (int64_t)mw[2];
   return TS_OK;
 }
 

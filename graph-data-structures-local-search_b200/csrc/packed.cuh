@@ -59,7 +59,7 @@ __device__ void slot_init(const DevGraph& g, const DevSolver<KeyT>& s, const int
   for (int32_t i = tid; i < m; i += T) { s.vg_in[i] = 0; s.tab_in[i] = 0; }
   for (int32_t j = tid; j < s.ldc; j += T) { s.vg_out[j] = 0; s.tab_out[j] = 0; }
   if (ST == S_WSWAP)
-    for (long long q = tid; q < (long long)s.n_row_blocks * Rows<ST>::R * s.ldc; q += T) s.W[q] = 0;
+    for (long long q = tid; q < (long long)s.n_row_blocks * Rows<ST>::R * s.ldc; q += T) w_set(s, q, 0);
   __syncthreads();
   long long acc = 0;
   if (PROB == P_MDP) {
@@ -99,7 +99,7 @@ __device__ void slot_init(const DevGraph& g, const DevSolver<KeyT>& s, const int
         const int2 e = g.adj[k];
         if (k > k0 && g.adj[k - 1].x == e.x) continue;  // first entry of a duplicated pair
         const int32_t p = s.pos[e.x];
-        if (p >= m) s.W[(long long)i * s.ldc + (p - m)] = e.y;
+        if (p >= m) w_set(s, (long long)i * s.ldc + (p - m), e.y);
       }
     }
   }

@@ -130,6 +130,7 @@ struct Req {
   int32_t num_pert = 1;
   bool plain = false, wide = false;
   int32_t cs = 1;
+  size_t smem = 16;  // packed: dynamic shared memory of one tile (tile_geometry)
   // device resources
   ts_graph* g = nullptr;
   cudaStream_t stream = nullptr;   // plain: the graph's and solver's stream
@@ -215,8 +216,7 @@ namespace {
 template <class KeyT>
 ts_status build_packed(Req& r, int32_t kind) {
   const int32_t n = r.n, m = r.m, delta = n - m;
-  const int R = rows_of(kind);
-  const int pc = pass_cols_of(kind);
+  const int R = rows_of(kind);  // WSwap matrix rows come in whole blocks of R
   const int64_t ldc = (delta + 3) & ~3;
   DevSolver<KeyT> s;
   std::memset(&s, 0, sizeof(s));
@@ -227,19 +227,16 @@ ts_status build_packed(Req& r, int32_t kind) {
   const int c1s[4] = {15, 30, 60, 120};
   for (int i = 0; i < 4; i++) s.c2_tab[i] = (int32_t)round(0.7 * c1s[i]);
   s.c2_fixed = (int32_t)round(0.7 * r.p.tenure);
-  s.n_row_blocks = (m + R - 1) / R;
-  const bool mdp_csr = kind == S_CSR && (r.p.problem == P_MDP || r.g->neg_w);
-  s.adj_mask = mdp_csr ? 1 : 0;
-  long long cols = ((delta + pc - 1) / pc) * (long long)pc;
-  if (kind == S_WSWAP) cols = std::min<long long>(cols, 8LL * pc);
-  if (mdp_csr) cols = std::min<long long>(cols, 16LL * pc);
-  const long long want = std::max<long long>(1, (r.cs + s.n_row_blocks - 1) / s.n_row_blocks);
-  long long c2 = (delta + want - 1) / want;
-  c2 = ((c2 + pc - 1) / pc) * pc;
-  cols = std::max<long long>(pc, std::min(cols, c2));
-  s.chunk_cols = (int32_t)cols;
-  s.n_chunks = (int32_t)((delta + cols - 1) / cols);
-  s.stage_bytes = (kind == S_CSR || kind == S_WSWAP) ? 0 : staging_bytes(r.g, R);
+  const TileGeom tg = tile_geometry(r.g, r.p.problem, m, sizeof(KeyT) == 8, r.cs, r.p.pass);
+  s.n_row_blocks = tg.n_row_blocks;
+  s.tile_rows = tg.rows;
+  s.fast = tg.fast;
+  s.fast_ecap = tg.fast_ecap;
+  s.adj_mask = tg.adj_mask;
+  s.chunk_cols = tg.chunk_cols;
+  s.n_chunks = tg.n_chunks;
+  s.stage_bytes = tg.stage_bytes;
+  r.smem = tg.smem;
   s.P = (int64_t)m * delta;
   const int64_t entries = r.g->entries;
   const int64_t events = r.p.problem == P_MAXBS ? r.p.max_iter / r.p.piter + 1 : 0;
@@ -524,11 +521,7 @@ void ts_server::round() {
         J->need_init = r.started ? 0 : 1;
         J->out = r.d_res;
         J->best_out = r.d_best;
-        const bool mdp_csr = r.kind == S_CSR && J->s.adj_mask;
-        size_t need = 16;
-        if (mdp_csr) need = 4 * (size_t)J->s.chunk_cols;
-        if (J->s.stage_bytes) need = (size_t)J->s.stage_bytes;
-        smem = std::max(smem, need);
+        smem = std::max(smem, r.smem);
       };
       if (wide) fill(reinterpret_cast<ServeJobDev<long long>*>(dst));
       else fill(reinterpret_cast<ServeJobDev<int32_t>*>(dst));

@@ -103,6 +103,57 @@ int32_t staging_bytes(const ts_graph* g, int R) {
   return (int32_t)std::min<int64_t>(cap, std::max<int64_t>(8 * 1024, head + R * row_bytes));
 }
 
+bool wswap_w16(const ts_graph* g) { return g->max_abs_w <= 32767; }
+
+TileGeom tile_geometry(const ts_graph* g, int32_t problem, int32_t m, bool wide, int64_t min_tiles,
+                       int32_t pass) {
+  TileGeom t;
+  const int kind = g->kind;
+  const int64_t delta = (int64_t)g->n - m;
+  int32_t ecap = 0;
+  if (!wide && kind != S_WSWAP && kind != S_CSR) {
+    // two 512-thread CTAs per SM: ~104 KB of index each
+    ecap = fast_ecap_for(kind, g->wpr, 104 * 1024);
+  }
+  // Below ~4 million pairs an iteration is a chain of latencies, and the
+  // per-row pass's smaller tiles spread it over more SMs.
+  const bool want_tile = pass == TS_PASS_TILE || (pass == TS_PASS_AUTO && (int64_t)m * delta >= (1LL << 22));
+  t.fast = (want_tile && !wide && kind != S_WSWAP && (kind == S_CSR || ecap > 0)) ? 1 : 0;
+  t.fast_ecap = t.fast ? ecap : 0;
+  t.rows = t.fast ? kFastRows : rows_of(kind);
+  t.n_row_blocks = (int32_t)((m + t.rows - 1) / t.rows);
+  const bool mdp_csr = kind == S_CSR && (problem == P_MDP || g->neg_w);
+  t.adj_mask = mdp_csr ? 1 : 0;
+  const int64_t pc = pass_cols_of(kind);
+  const int64_t full = ((delta + pc - 1) / pc) * pc;
+  int64_t max_cols = full;
+  if (kind == S_WSWAP) max_cols = 8 * pc;
+  if (mdp_csr) max_cols = 16 * pc;  // the per-column mask stays within 64 KB
+  if (t.fast && kind != S_CSR) {
+    // a heavy row's column bitmap reuses the index memory: 8 columns per byte
+    const int64_t fit = (int64_t)fast_layout(kind, ecap, g->wpr).total * 8;
+    max_cols = std::max<int64_t>(pc, std::min<int64_t>(max_cols, (fit / pc) * pc));
+  }
+  const int64_t want_chunks = std::max<int64_t>(1, (min_tiles + t.n_row_blocks - 1) / t.n_row_blocks);
+  int64_t cols = (delta + want_chunks - 1) / want_chunks;
+  cols = ((cols + pc - 1) / pc) * pc;
+  cols = std::max<int64_t>(pc, std::min<int64_t>(cols, max_cols));
+  t.chunk_cols = (int32_t)cols;
+  t.n_chunks = (int32_t)((delta + cols - 1) / cols);
+  t.stage_bytes = 0;
+  if (kind == S_CSR) {
+    t.smem = mdp_csr ? sizeof(uint32_t) * (size_t)cols : 16;
+  } else if (kind == S_WSWAP) {
+    t.smem = 16;
+  } else if (t.fast) {
+    t.smem = fast_layout(kind, ecap, g->wpr).total;
+  } else {
+    t.stage_bytes = staging_bytes(g, t.rows);
+    t.smem = (size_t)t.stage_bytes;
+  }
+  return t;
+}
+
 namespace {
 
 constexpr int kInitTPB = 256;
@@ -163,7 +214,7 @@ __global__ void k_init_wswap(const DevGraph g, const DevSolver<KeyT> s) {
       const int2 e = g.adj[k];
       if (k > a0 && g.adj[k - 1].x == e.x) continue;
       const int32_t p = s.pos[e.x];
-      if (p >= s.m) s.W[(long long)i * s.ldc + (p - s.m)] = e.y;
+      if (p >= s.m) w_set(s, (long long)i * s.ldc + (p - s.m), e.y);
     }
   }
 }
@@ -268,8 +319,6 @@ int64_t wave_cols(int64_t delta, int64_t rows, int64_t pc, int64_t lo, int64_t c
   return pick;
 }
 
-int rows_per_tile(int kind) { return rows_of(kind); }
-
 }  // namespace
 }  // namespace tsb
 
@@ -283,7 +332,7 @@ struct ts_solver {
   int64_t P = 0;
   int R = 0;
   int32_t n_row_blocks = 0, n_chunks = 0, chunk_cols = 0, stage_bytes = 0;
-  int32_t adj_mask = 0;
+  int32_t adj_mask = 0, fast = 0, fast_ecap = 0, w16 = 0;
   size_t dyn_smem = 0;
   int grid = 0;
   int32_t num_pert = 1;
@@ -315,6 +364,10 @@ struct ts_solver {
     s.n_row_blocks = n_row_blocks; s.n_chunks = n_chunks; s.chunk_cols = chunk_cols;
     s.stage_bytes = stage_bytes;
     s.adj_mask = adj_mask;
+    s.tile_rows = R;
+    s.fast = fast;
+    s.fast_ecap = fast_ecap;
+    s.w16 = w16;
     s.P = P;
     s.sol_in = sol_in.as<int32_t>(); s.sol_out = sol_out.as<int32_t>();
     s.vg_in = vg_in.as<KeyT>(); s.vg_out = vg_out.as<KeyT>();
@@ -510,7 +563,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   const int32_t n = g->n;
   const int32_t m = p->problem == TS_PROBLEM_MDP ? p->m : n / 2;
   if (m < 1 || m >= n) { set_error("ts_solver_create: need 1 <= m < n"); return TS_ERR_INVALID_ARG; }
-  if (p->max_iter < 0 || p->piter < 1 || p->gamma < 0 || p->maxt < 1 ||
+  if (p->max_iter < 0 || p->piter < 1 || p->gamma < 0 || p->maxt < 1 || p->pass < 0 || p->pass > 2 ||
       (p->tenure_policy != TS_TENURE_REF && p->tenure_policy != TS_TENURE_FIXED) || p->tenure < 0) {
     set_error("ts_solver_create: bad parameters");
     return TS_ERR_INVALID_ARG;
@@ -526,30 +579,21 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   s->P = (int64_t)m * s->delta;
   // 32-bit pair keys while every gain stays within +-2^30.
   s->wide = 4 * g->max_wdeg >= (1LL << 30);
-  s->R = rows_per_tile(g->kind);
-  s->n_row_blocks = (m + s->R - 1) / s->R;
-  // Tile geometry.  Staged structures (BB/Hash/Bitset) and MaxBS CSR span the
-  // whole row width once there are enough row blocks, so each CTA stages or
-  // joins its rows once per iteration; masked CSR (MDP, or MaxBS with a
-  // negative weight) keeps a per-column mask in shared memory (<= 16384
-  // columns); WSwap has no per-CTA setup.
-  const bool mdp_csr = g->kind == S_CSR && (p->problem == TS_PROBLEM_MDP || g->neg_w);
-  s->adj_mask = mdp_csr ? 1 : 0;
-  const int64_t pc = pass_cols_of(g->kind);  // columns one pass of the CTA covers
-  const int64_t full = ((s->delta + pc - 1) / pc) * pc;
-  int64_t max_cols = full;
-  if (g->kind == S_WSWAP) max_cols = 8 * pc;
-  if (mdp_csr) max_cols = 16 * pc;
-  // Tiles per iteration: the staged structures (per-tile row staging, uneven
-  // rows) balance better over many column chunks; CSR and WSwap prefer few
-  // wide tiles.  One CTA per tile; the hardware schedules them.
+  // Tiles per iteration: the index structures balance their uneven rows
+  // over many tiles; CSR and WSwap prefer few wide ones.  One CTA per tile;
+  // the hardware schedules them.
   const bool staged = g->kind != S_CSR && g->kind != S_WSWAP;
-  const int64_t min_grid = staged ? 8 * 148 : (g->kind == S_WSWAP ? 4 * 148 : 2 * 148);
-  const int64_t want_chunks = std::max<int64_t>(1, (min_grid + s->n_row_blocks - 1) / s->n_row_blocks);
-  int64_t cols = (s->delta + want_chunks - 1) / want_chunks;
-  cols = ((cols + pc - 1) / pc) * pc;
-  cols = std::max<int64_t>(pc, std::min<int64_t>(cols, max_cols));
+  const int64_t min_grid = staged ? 4 * 148 : (g->kind == S_WSWAP ? 4 * 148 : 2 * 148);
+  const TileGeom tg = tile_geometry(g, p->problem, m, s->wide, min_grid, p->pass);
+  s->R = tg.rows;
+  s->w16 = g->kind == S_WSWAP && wswap_w16(g) ? 1 : 0;
+  s->fast = tg.fast;
+  s->fast_ecap = tg.fast_ecap;
+  s->n_row_blocks = tg.n_row_blocks;
+  s->adj_mask = tg.adj_mask;
+  int64_t cols = tg.chunk_cols;
   if (g->kind == S_WSWAP) {
+    const int64_t pc = pass_cols_of(g->kind);
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess) {
       cudaGetLastError();
@@ -561,16 +605,8 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   s->chunk_cols = (int32_t)cols;
   s->n_chunks = (int32_t)((s->delta + cols - 1) / cols);
   s->grid = s->n_row_blocks * s->n_chunks;
-  if (g->kind == S_CSR) {
-    s->stage_bytes = 0;
-    s->dyn_smem = mdp_csr ? sizeof(uint32_t) * (size_t)s->chunk_cols : 16;
-  } else if (g->kind == S_WSWAP) {
-    s->stage_bytes = 0;
-    s->dyn_smem = 16;
-  } else {
-    s->stage_bytes = staging_bytes(g, s->R);
-    s->dyn_smem = s->stage_bytes;
-  }
+  s->stage_bytes = tg.stage_bytes;
+  s->dyn_smem = tg.smem;
   const int32_t g_eff = std::min(p->gamma, n);
   s->num_pert = std::max(1, g_eff / 2);  // GPU-MAXBS-CSR.cu:433-434
   int64_t pert_moves = p->problem == TS_PROBLEM_MAXBS ? (p->max_iter / p->piter + 1) * s->num_pert : 0;
@@ -597,7 +633,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   if (g->kind == S_WSWAP) {
     // Padded to whole row blocks so a tile never reads past the matrix.
     size_t rows = (size_t)s->n_row_blocks * s->R;
-    A(s->W, sizeof(int32_t) * rows * (size_t)s->ldc, "alloc WSwap matrix");
+    A(s->W, (s->w16 ? sizeof(int16_t) : sizeof(int32_t)) * rows * (size_t)s->ldc, "alloc WSwap matrix");
   }
   if (g->kind == S_CSR) A(s->cpos, sizeof(int32_t) * (size_t)std::max<int64_t>(1, g->entries), "alloc cpos");
   if (rc == TS_OK) {
@@ -941,7 +977,7 @@ ts_status ts_solver_info_get(const ts_solver* s, ts_solver_info* out) {
   out->threads = tpb_of(s->g->kind);
   out->dyn_smem_bytes = (int32_t)s->dyn_smem;
   out->key_bytes = s->wide ? 8 : 4;
-  out->w_bytes = s->g->kind == S_WSWAP ? 4 : 0;
+  out->w_bytes = s->g->kind == S_WSWAP ? (s->w16 ? 2 : 4) : 0;
   return TS_OK;
 }
 

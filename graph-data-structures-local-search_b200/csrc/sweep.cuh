@@ -25,6 +25,7 @@
 #pragma once
 #include <climits>
 #include <cstdint>
+#include <type_traits>
 
 #include "ts_internal.cuh"
 
@@ -34,10 +35,12 @@ constexpr int kColsPerLane = 4;
 constexpr int kMaxTPB = 512;
 // Threads per CTA: the bitmap structures stage ~n/8 bytes per row, so they run
 // one large CTA per SM and need more warps in it to hide shared-memory latency.
-template <int ST> struct Tpb { static constexpr int v = 256; };
-template <> struct Tpb<S_BITSET> { static constexpr int v = 512; };
-template <> struct Tpb<S_BITSET_BB> { static constexpr int v = 512; };
-__host__ __device__ inline int tpb_of(int st) { return (st == S_BITSET || st == S_BITSET_BB) ? 512 : 256; }
+// The index structures (Hash, BB, bitmaps) build a shared-memory index per
+// tile and run two 512-thread CTAs per SM.
+template <int ST> struct Tpb { static constexpr int v = 512; };
+template <> struct Tpb<S_CSR> { static constexpr int v = 256; };
+template <> struct Tpb<S_WSWAP> { static constexpr int v = 256; };
+__host__ __device__ inline int tpb_of(int st) { return (st == S_CSR || st == S_WSWAP) ? 256 : 512; }
 __host__ __device__ inline int pass_cols_of(int st) { return tpb_of(st) * kColsPerLane; }
 
 template <int ST> struct Rows { static constexpr int R = 16; };
@@ -50,7 +53,9 @@ template <> struct Rows<S_BITSET_BB> { static constexpr int R = 8; };
 // column loads shared by fewer rows notwithstanding.
 template <> struct Rows<S_HASH> { static constexpr int R = 4; };
 template <> struct Rows<S_BB> { static constexpr int R = 4; };
-// Rows per tile by structure id (host side of the traits above).
+constexpr int kMaxTileRows = 32;
+// Rows per tile of the pass with per-row registers (64-bit keys, or a graph
+// too large for the fast pass's index), by structure id.
 __host__ __device__ inline int rows_of(int st) {
   return st == S_CSR ? Rows<S_CSR>::R
        : st == S_BITSET ? Rows<S_BITSET>::R
@@ -76,6 +81,20 @@ template <int PROB, class KeyT>
 __device__ __forceinline__ KeyT pair_gain(KeyT rowv, KeyT colv, int32_t w) {
   if (PROB == P_MDP) return colv - rowv - (KeyT)w;  // vg[v] - vg[u] - w(u,v)
   return rowv + colv + (KeyT)2 * (KeyT)w;           // vg[u] + vg[v] + 2 w(u,v)
+}
+
+// WSwap sweep: the gain split into a column part, maximised per row over the
+// thread's columns, and the row's own term added once afterwards:
+// MaxBS vg[u] + (vg[v] + 2w), MDP (vg[v] - w) - vg[u].
+template <int PROB, class KeyT>
+__device__ __forceinline__ KeyT wsw_col_term(KeyT colv, int32_t w) {
+  if (PROB == P_MDP) return colv - (KeyT)w;
+  return colv + (KeyT)2 * (KeyT)w;
+}
+template <int PROB, class KeyT>
+__device__ __forceinline__ KeyT wsw_row_term(KeyT rowv, KeyT col_term) {
+  if (PROB == P_MDP) return col_term - rowv;
+  return rowv + col_term;
 }
 
 __device__ __forceinline__ bool allowed(bool row_tabu, bool col_tabu, long long x, long long D) {
@@ -148,6 +167,42 @@ template <bool PERSIST>
 __device__ __forceinline__ int32_t ld_w1(const int32_t* p) {
   if constexpr (PERSIST) return __ldcg(p);
   else return *p;
+}
+// 16-bit matrix: four weights of a row in one 8-byte load, same policies;
+// kept packed until used (unpack_w16) so all rows' loads stay in flight.
+template <bool PERSIST>
+__device__ __forceinline__ int2 ld_w4_16(const int16_t* p) {
+  int2 r;
+  if constexpr (PERSIST) {
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
+        "ld.global.L1::no_allocate.L2::cache_hint.v2.s32 {%0,%1}, [%2], pol;\n\t}"
+        : "=r"(r.x), "=r"(r.y)
+        : "l"(p));
+  } else {
+    r = __ldcs(reinterpret_cast<const int2*>(p));
+  }
+  return r;
+}
+__device__ __forceinline__ int4 unpack_w16(int2 r) {
+  return make_int4((r.x << 16) >> 16, r.x >> 16, (r.y << 16) >> 16, r.y >> 16);
+}
+
+// WSwap matrix element access for either element width.
+template <bool PERSIST, class KeyT>
+__device__ __forceinline__ int32_t w_get(const DevSolver<KeyT>& s, long long at) {
+  if (s.w16) {
+    const int16_t* W16 = reinterpret_cast<const int16_t*>(s.W);
+    if constexpr (PERSIST) return (int32_t)__ldcg(W16 + at);
+    else return (int32_t)W16[at];
+  }
+  return ld_w1<PERSIST>(s.W + at);
+}
+template <class KeyT>
+__device__ __forceinline__ void w_set(const DevSolver<KeyT>& s, long long at, int32_t v) {
+  if (s.w16) reinterpret_cast<int16_t*>(s.W)[at] = (int16_t)v;
+  else s.W[at] = v;
 }
 
 // Column loads: 4 contiguous columns per lane (16 B aligned since ldc % 4 == 0).
@@ -291,7 +346,7 @@ __device__ __forceinline__ int32_t lite_lookup(const unsigned char* base, const 
 template <int ST, class KeyT, bool PERSIST>
 __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSolver<KeyT>& s,
                                                  int32_t row, int32_t col, int32_t u, int32_t v) {
-  if (ST == S_WSWAP) return ld_w1<PERSIST>(s.W + (long long)row * s.ldc + col);
+  if (ST == S_WSWAP) return w_get<PERSIST>(s, (long long)row * s.ldc + col);
   const long long st = g.rowptr[u];
   const int32_t deg = (int32_t)(g.rowptr[u + 1] - st);
   const int32_t* ck = reinterpret_cast<const int32_t*>(g.adj + st);
@@ -305,6 +360,10 @@ __device__ __forceinline__ int32_t global_lookup(const DevGraph& g, const DevSol
   if (!bit_test(g.bits + (long long)u * g.wpr, v)) return 0;
   return ST == S_BITSET ? scan_first<2>(ck, ck + 1, deg, v) : bb_lower<2>(ck, ck + 1, deg, v);
 }
+
+}  // namespace tsb
+#include "fast.cuh"
+namespace tsb {
 
 template <class KeyT>
 __device__ __forceinline__ KeyT* vg_at(const DevSolver<KeyT>& s, int32_t p) {
@@ -384,19 +443,34 @@ __device__ long long apply_swap(const DevGraph& g, const DevSolver<KeyT>& s, int
       if (ST == S_CSR) s.cpos[rv[j]] = from_u ? m + jv : iu;  // new position of u / v
       const bool first = prev[j] != z;
       if (PROB == P_MAXBS && from_u && z == v && first) sh.wuv = w;
-      if (ST == S_WSWAP && first && z != (from_u ? u : v)) {
+      if (ST == S_WSWAP && z != u && z != v) {
         // Row iu now describes v, column jv now describes u
-        // (updateVertexEdgeGain, GPU-MDP-WSwap.cu:535-560).  Self-loop entries
-        // (kept by the MaxBS loader) are skipped: the reference's patch would fold
-        // them into W[iu][jv], and W must keep returning the CSR lookup's w(u,v).
-        if (from_u && z != v) {
-          if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], -w);
-          else atomicAdd(&s.W[(long long)p * s.ldc + jv], w);
-        } else if (!from_u && z != u) {
-          if (p >= m) atomicAdd(&s.W[(long long)iu * s.ldc + (p - m)], w);
-          else atomicAdd(&s.W[(long long)p * s.ldc + jv], -w);
-        }
+        // (updateVertexEdgeGain, GPU-MDP-WSwap.cu:535-560).  First the
+        // entries that stop being edges are cleared: row iu at u's outside
+        // neighbours, column jv at v's inside neighbours ...
+        if (from_u && p >= m) w_set(s, (long long)iu * s.ldc + (p - m), 0);
+        if (!from_u && p < m) w_set(s, (long long)p * s.ldc + jv, 0);
       }
+    }
+  }
+  if (ST == S_WSWAP) {
+    // ... then the new edges are set: row iu at v's outside neighbours,
+    // column jv at u's inside neighbours, each with the first entry of a
+    // duplicated pair.  The element (iu, jv) -- w(u, v) either way -- and
+    // self-loop entries (kept by the MaxBS loader) are left alone, so W keeps
+    // returning the CSR lookup's w(u, v).  Plain stores: every element is
+    // written by one entry, after the barrier that ends the clearing.
+    __syncthreads();
+    for (int32_t k = threadIdx.x; k < total; k += blockDim.x) {
+      const bool from_u = k < nu;
+      const long long at = from_u ? su + k : sv + (k - nu);
+      const long long rs = from_u ? su : sv;
+      const int2 e = g.adj[at];
+      if (e.x == u || e.x == v) continue;
+      if (at != rs && g.adj[at - 1].x == e.x) continue;
+      const int32_t p = s.pos[e.x];
+      if (!from_u && p >= m) w_set(s, (long long)iu * s.ldc + (p - m), e.y);
+      if (from_u && p < m) w_set(s, (long long)p * s.ldc + jv, e.y);
     }
   }
   __syncthreads();
@@ -555,6 +629,12 @@ template <int PROB, int ST, class KeyT, bool PERSIST>
 __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
                           long long D64, int rb, int ch, long long& out_key, long long& out_idx,
                           TailShared& sh, long long floor_key = LLONG_MIN) {
+  if constexpr (std::is_same<KeyT, int32_t>::value && ST != S_WSWAP) {
+    if (mode == 0 && s.fast) {
+      tile_fast<PROB, ST, PERSIST>(g, s, iter, D64, rb, ch, out_key, out_idx);
+      return;
+    }
+  }
   constexpr int R = Rows<ST>::R;
   constexpr int TPB = Tpb<ST>::v;
   using Lim = KeyLim<KeyT>;
@@ -562,9 +642,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
   const int tid = threadIdx.x, lane = tid & 31;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ KeyT s_rv[R];
-  __shared__ int32_t s_ru[R];
-  __shared__ int32_t s_rtab[R];
+  __shared__ KeyT s_rv[kMaxTileRows];
+  __shared__ int32_t s_ru[kMaxTileRows];
+  __shared__ int32_t s_rtab[kMaxTileRows];
   __shared__ KeyT s_rowbest[R];
   __shared__ RowDesc s_desc[R];
   __shared__ long long s_rstart[R];
@@ -573,17 +653,20 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
   __shared__ int32_t s_rstar;
   __shared__ uint32_t s_cmin;
 
-  const int32_t r0 = rb * R;
-  const int32_t nr = min(R, s.m - r0);
+  // the exact pass takes the solver's tile height (the fast pass's 32 rows
+  // when that pass is on); the per-row-register pass below is compiled for R
+  const int Rt = mode == 1 ? s.tile_rows : R;
+  const int32_t r0 = rb * Rt;
+  const int32_t nr = min(Rt, s.m - r0);
   const int32_t c0 = ch * s.chunk_cols;
   const int32_t c_end = min(c0 + s.chunk_cols, s.delta);
 
-  if (tid < R) {
+  if (tid < Rt) {
     const bool ok = tid < nr;
     s_rv[tid] = ok ? ld_st<PERSIST>(s.vg_in + r0 + tid) : (KeyT)0;
     s_ru[tid] = ok ? ld_st<PERSIST>(s.sol_in + r0 + tid) : 0;
     s_rtab[tid] = ok ? (ld_st<PERSIST>(s.tab_in + r0 + tid) > iter) : 0;
-    s_rowbest[tid] = Lim::none;
+    if (tid < R) s_rowbest[tid] = Lim::none;
   }
   __syncthreads();
 
@@ -818,202 +901,240 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
     }
 
     const int passes = s.chunk_cols / (TPB * kColsPerLane);
-    for (int pass = 0; pass < passes; pass++) {
-      const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
-      const bool lane_on = cb < c_end;
-      if (ST == S_BITSET || ST == S_BITSET_BB) {
-        // the bitmap paths vote across the warp: leave the loop together
-        if (__all_sync(0xffffffffu, !lane_on)) break;
-      } else if (!lane_on) {
-        break;
-      }
-      KeyT cv[4];
-      int32_t ct4[4];
-      bool valid[4], ct[4];
-      if (ST == S_WSWAP) {
-        // Issue every row's W load of this pass before using any: the matrix
-        // streams from HBM once per iteration.
-        int4 wv[R];
-#pragma unroll
-        for (int r = 0; r < R; r++)
-          wv[r] = ld_w4<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + cb);
-        load4<PERSIST>(s.vg_out + cb, cv);
-        load4<PERSIST>(s.tab_out + cb, ct4);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          valid[q] = cb + q < c_end;
-          ct[q] = ct4[q] > iter;
+    // The WSwap matrix element width is a compile-time choice of the pass
+    // loop, so each width gets its own register allocation.
+    auto sweep_passes = [&](auto w16_tag) {
+      constexpr bool W16 = decltype(w16_tag)::value;
+      for (int pass = 0; pass < passes; pass++) {
+        const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
+        const bool lane_on = cb < c_end;
+        if (ST == S_BITSET || ST == S_BITSET_BB) {
+          // the bitmap paths vote across the warp: leave the loop together
+          if (__all_sync(0xffffffffu, !lane_on)) break;
+        } else if (!lane_on) {
+          break;
         }
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          const KeyT t = s_rv[r];
-          const int32_t w4[4] = {wv[r].x, wv[r].y, wv[r].z, wv[r].w};
-#pragma unroll
+        KeyT cv[4];
+        int32_t ct4[4];
+        bool valid[4], ct[4];
+        if (ST == S_WSWAP) {
+          // Issue every row's W load of this pass before using any: the matrix
+          // streams from HBM once per iteration.
+          int4 wv[R];
+          int2 wp[R];
+          if constexpr (W16) {
+            const int16_t* W16p = reinterpret_cast<const int16_t*>(s.W);
+  #pragma unroll
+            for (int r = 0; r < R; r++) wp[r] = ld_w4_16<PERSIST>(W16p + (long long)(r0 + r) * s.ldc + cb);
+          } else {
+  #pragma unroll
+            for (int r = 0; r < R; r++) wv[r] = ld_w4<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + cb);
+          }
+          load4<PERSIST>(s.vg_out + cb, cv);
+          load4<PERSIST>(s.tab_out + cb, ct4);
+  #pragma unroll
           for (int q = 0; q < 4; q++) {
-            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], w4[q]);
-            if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+            valid[q] = cb + q < c_end;
+            ct[q] = ct4[q] > iter;
           }
-        }
-        continue;
-      }
-      if (lane_on) {
-        load4<PERSIST>(s.vg_out + cb, cv);
-        load4<PERSIST>(s.tab_out + cb, ct4);
-      } else {
-#pragma unroll
-        for (int q = 0; q < 4; q++) { cv[q] = 0; ct4[q] = 0; }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        valid[q] = lane_on && cb + q < c_end;
-        ct[q] = ct4[q] > iter;
-      }
-      if (ST == S_CSR) {
-        uint32_t mk[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          mk[q] = valid[q] ? (masked ? s_mask[cb + q - c0] : 0u) : 0xffffffffu;
-          if (valid[q] && ct[q]) {
-            // Tabu column: a pair is allowed only when aspirated (gain > best - cur).
-#pragma unroll
-            for (int r = 0; r < R; r++)
-              if (!(pair_gain<PROB, KeyT>(s_rv[r], cv[q], 0) > D)) mk[q] |= 1u << r;
-          }
-        }
-        if ((mk[0] | mk[1] | mk[2] | mk[3]) == 0u) {
-#pragma unroll
+          // best[r] holds the row's maximum of the column part of the gain
+          // (MaxBS vg[v] + 2w, MDP vg[v] - w); the row's own term is added
+          // once per row after the sweep (wsw_row_term)
+          const bool plain4 = valid[0] && valid[1] && valid[2] && valid[3] && !(ct[0] || ct[1] || ct[2] || ct[3]);
+  #pragma unroll
           for (int r = 0; r < R; r++) {
-            const KeyT t = s_rv[r];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-              const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], 0);
-              best[r] = x > best[r] ? x : best[r];
-            }
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < R; r++) {
-            const KeyT t = s_rv[r];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-              const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], 0);
-              if (!((mk[q] >> r) & 1u)) best[r] = x > best[r] ? x : best[r];
-            }
-          }
-        }
-      } else {
-        int32_t vx[4] = {0, 0, 0, 0};
-        if (lane_on) load4<PERSIST>(s.sol_out + cb, vx);
-        if ((ST == S_BITSET || ST == S_BITSET_BB) && bm_staged) {
-          // Lean bitmap path.  Columns past the chunk read word 0 of the row
-          // and are masked by `valid`.  Pairs that hit
-          // (rare: deg / n) get their weight from the row in a warp-uniform
-          // branch; when every lane's four columns are valid and non-tabu the
-          // gain goes straight into the maximum.
-          uint32_t wofs[4], bsh[4];
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const uint32_t vv = valid[q] ? (uint32_t)vx[q] : 0u;  // in-bounds word for any lane
-            wofs[q] = (vv >> 5) << 2;
-            bsh[q] = vv & 31u;
-          }
-          const bool simple = valid[0] && valid[1] && valid[2] && valid[3] && !(ct[0] || ct[1] || ct[2] || ct[3]);
-          const bool wsimple = __all_sync(0xffffffffu, simple);
-#pragma unroll
-          for (int r = 0; r < R; r++) {
-            if (r >= nr) continue;
-            const KeyT t = s_rv[r];
-            const unsigned char* rb = smem_raw + rbase[r];
-            bool hq[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-              hq[q] = valid[q] && ((*reinterpret_cast<const uint32_t*>(rb + wofs[q]) >> bsh[q]) & 1u);
-            int32_t wq[4] = {0, 0, 0, 0};
-            unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
-            if (any) {
-              const RowDesc d = s_desc[r];
-              if (ST == S_BITSET) {
-                // each hit resolved by the whole warp scanning the row 32 entries at a time
-                while (any) {
-                  const int L = __ffs(any) - 1;
-                  any &= any - 1;
-#pragma unroll
-                  for (int q = 0; q < 4; q++) {
-                    const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
-                    if (hv >= 0) {
-                      const int32_t ww = warp_scan_first(d, hv);
-                      if (lane == L) wq[q] = ww;
-                    }
-                  }
-                }
-              } else {
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                  if (hq[q]) wq[q] = bb_lower(d, vx[q]);
+            if constexpr (W16) wv[r] = unpack_w16(wp[r]);
+            const int32_t w4[4] = {wv[r].x, wv[r].y, wv[r].z, wv[r].w};
+            if (plain4) {
+              KeyT m = wsw_col_term<PROB, KeyT>(cv[0], w4[0]);
+  #pragma unroll
+              for (int q = 1; q < 4; q++) {
+                const KeyT y = wsw_col_term<PROB, KeyT>(cv[q], w4[q]);
+                m = y > m ? y : m;
               }
-            }
-            if (wsimple) {
-#pragma unroll
-              for (int q = 0; q < 4; q++) {
-                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
-                best[r] = x > best[r] ? x : best[r];
-              }
+              best[r] = m > best[r] ? m : best[r];
             } else {
-#pragma unroll
+              const KeyT t = s_rv[r];
+  #pragma unroll
               for (int q = 0; q < 4; q++) {
-                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
-                if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+                const KeyT y = wsw_col_term<PROB, KeyT>(cv[q], w4[q]);
+                const KeyT x = wsw_row_term<PROB, KeyT>(t, y);
+                if (valid[q] && (!ct[q] || x > D)) best[r] = y > best[r] ? y : best[r];
               }
             }
           }
           continue;
         }
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          if (r >= nr) continue;
-          const KeyT t = s_rv[r];
-          int32_t wq[4];
-          if (ST == S_BB && s_lite[r].x != kNotStaged) {
-            const uint4 L = s_lite[r];  // the same for the whole CTA: a uniform branch
-#pragma unroll
-            for (int q = 0; q < 4; q++) wq[q] = valid[q] ? lite_lookup<ST>(smem_raw, L, vx[q]) : 0;
-          } else if (ST == S_BITSET) {
-            const RowDesc d = s_desc[r];
-            // Bit test per pair; each hit is resolved by the whole warp
-            // scanning the row 32 entries at a time (first match by ballot).
-            bool hq[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-              hq[q] = valid[q] && bit_test(d.bits, vx[q]);
-              wq[q] = 0;
+        if (lane_on) {
+          load4<PERSIST>(s.vg_out + cb, cv);
+          load4<PERSIST>(s.tab_out + cb, ct4);
+        } else {
+  #pragma unroll
+          for (int q = 0; q < 4; q++) { cv[q] = 0; ct4[q] = 0; }
+        }
+  #pragma unroll
+        for (int q = 0; q < 4; q++) {
+          valid[q] = lane_on && cb + q < c_end;
+          ct[q] = ct4[q] > iter;
+        }
+        if (ST == S_CSR) {
+          uint32_t mk[4];
+  #pragma unroll
+          for (int q = 0; q < 4; q++) {
+            mk[q] = valid[q] ? (masked ? s_mask[cb + q - c0] : 0u) : 0xffffffffu;
+            if (valid[q] && ct[q]) {
+              // Tabu column: a pair is allowed only when aspirated (gain > best - cur).
+  #pragma unroll
+              for (int r = 0; r < R; r++)
+                if (!(pair_gain<PROB, KeyT>(s_rv[r], cv[q], 0) > D)) mk[q] |= 1u << r;
             }
-            unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
-            while (any) {
-              const int L = __ffs(any) - 1;
-              any &= any - 1;
-#pragma unroll
+          }
+          if ((mk[0] | mk[1] | mk[2] | mk[3]) == 0u) {
+  #pragma unroll
+            for (int r = 0; r < R; r++) {
+              const KeyT t = s_rv[r];
+  #pragma unroll
               for (int q = 0; q < 4; q++) {
-                const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
-                if (hv >= 0) {
-                  const int32_t ww = warp_scan_first(d, hv);
-                  if (lane == L) wq[q] = ww;
-                }
+                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], 0);
+                best[r] = x > best[r] ? x : best[r];
               }
             }
           } else {
-            const RowDesc d = s_desc[r];
-#pragma unroll
-            for (int q = 0; q < 4; q++) wq[q] = valid[q] ? staged_lookup<ST>(d, vx[q]) : 0;
+  #pragma unroll
+            for (int r = 0; r < R; r++) {
+              const KeyT t = s_rv[r];
+  #pragma unroll
+              for (int q = 0; q < 4; q++) {
+                const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], 0);
+                if (!((mk[q] >> r) & 1u)) best[r] = x > best[r] ? x : best[r];
+              }
+            }
           }
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
-            if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+        } else {
+          int32_t vx[4] = {0, 0, 0, 0};
+          if (lane_on) load4<PERSIST>(s.sol_out + cb, vx);
+          if ((ST == S_BITSET || ST == S_BITSET_BB) && bm_staged) {
+            // Lean bitmap path.  Columns past the chunk read word 0 of the row
+            // and are masked by `valid`.  Pairs that hit
+            // (rare: deg / n) get their weight from the row in a warp-uniform
+            // branch; when every lane's four columns are valid and non-tabu the
+            // gain goes straight into the maximum.
+            uint32_t wofs[4], bsh[4];
+  #pragma unroll
+            for (int q = 0; q < 4; q++) {
+              const uint32_t vv = valid[q] ? (uint32_t)vx[q] : 0u;  // in-bounds word for any lane
+              wofs[q] = (vv >> 5) << 2;
+              bsh[q] = vv & 31u;
+            }
+            const bool simple = valid[0] && valid[1] && valid[2] && valid[3] && !(ct[0] || ct[1] || ct[2] || ct[3]);
+            const bool wsimple = __all_sync(0xffffffffu, simple);
+  #pragma unroll
+            for (int r = 0; r < R; r++) {
+              if (r >= nr) continue;
+              const KeyT t = s_rv[r];
+              const unsigned char* rb = smem_raw + rbase[r];
+              bool hq[4];
+  #pragma unroll
+              for (int q = 0; q < 4; q++)
+                hq[q] = valid[q] && ((*reinterpret_cast<const uint32_t*>(rb + wofs[q]) >> bsh[q]) & 1u);
+              int32_t wq[4] = {0, 0, 0, 0};
+              unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
+              if (any) {
+                const RowDesc d = s_desc[r];
+                if (ST == S_BITSET) {
+                  // each hit resolved by the whole warp scanning the row 32 entries at a time
+                  while (any) {
+                    const int L = __ffs(any) - 1;
+                    any &= any - 1;
+  #pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                      const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
+                      if (hv >= 0) {
+                        const int32_t ww = warp_scan_first(d, hv);
+                        if (lane == L) wq[q] = ww;
+                      }
+                    }
+                  }
+                } else {
+  #pragma unroll
+                  for (int q = 0; q < 4; q++)
+                    if (hq[q]) wq[q] = bb_lower(d, vx[q]);
+                }
+              }
+              if (wsimple) {
+  #pragma unroll
+                for (int q = 0; q < 4; q++) {
+                  const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
+                  best[r] = x > best[r] ? x : best[r];
+                }
+              } else {
+  #pragma unroll
+                for (int q = 0; q < 4; q++) {
+                  const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
+                  if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+                }
+              }
+            }
+            continue;
+          }
+  #pragma unroll
+          for (int r = 0; r < R; r++) {
+            if (r >= nr) continue;
+            const KeyT t = s_rv[r];
+            int32_t wq[4];
+            if (ST == S_BB && s_lite[r].x != kNotStaged) {
+              const uint4 L = s_lite[r];  // the same for the whole CTA: a uniform branch
+  #pragma unroll
+              for (int q = 0; q < 4; q++) wq[q] = valid[q] ? lite_lookup<ST>(smem_raw, L, vx[q]) : 0;
+            } else if (ST == S_BITSET) {
+              const RowDesc d = s_desc[r];
+              // Bit test per pair; each hit is resolved by the whole warp
+              // scanning the row 32 entries at a time (first match by ballot).
+              bool hq[4];
+  #pragma unroll
+              for (int q = 0; q < 4; q++) {
+                hq[q] = valid[q] && bit_test(d.bits, vx[q]);
+                wq[q] = 0;
+              }
+              unsigned any = __ballot_sync(0xffffffffu, hq[0] | hq[1] | hq[2] | hq[3]);
+              while (any) {
+                const int L = __ffs(any) - 1;
+                any &= any - 1;
+  #pragma unroll
+                for (int q = 0; q < 4; q++) {
+                  const int32_t hv = __shfl_sync(0xffffffffu, hq[q] ? vx[q] : -1, L);
+                  if (hv >= 0) {
+                    const int32_t ww = warp_scan_first(d, hv);
+                    if (lane == L) wq[q] = ww;
+                  }
+                }
+              }
+            } else {
+              const RowDesc d = s_desc[r];
+  #pragma unroll
+              for (int q = 0; q < 4; q++) wq[q] = valid[q] ? staged_lookup<ST>(d, vx[q]) : 0;
+            }
+  #pragma unroll
+            for (int q = 0; q < 4; q++) {
+              const KeyT x = pair_gain<PROB, KeyT>(t, cv[q], wq[q]);
+              if (valid[q] && (!ct[q] || x > D)) best[r] = x > best[r] ? x : best[r];
+            }
           }
         }
       }
+    };
+    if constexpr (ST == S_WSWAP) {
+      if (s.w16) sweep_passes(std::true_type{});
+      else sweep_passes(std::false_type{});
+    } else {
+      sweep_passes(std::false_type{});
     }
 
+    if (ST == S_WSWAP) {
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (best[r] != Lim::none) best[r] = wsw_row_term<PROB, KeyT>(s_rv[r], best[r]);
+    }
     // Per-row block maximum.
 #pragma unroll
     for (int r = 0; r < R; r++) {
@@ -1065,7 +1186,7 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
               // exceeds its exact gain, so it cannot equal the row maximum alone.
               if (masked && ((s_mask[c - c0] >> r) & 1u)) continue;
             } else if (ST == S_WSWAP) {
-              w = ld_w1<PERSIST>(s.W + (long long)(r0 + r) * s.ldc + c);
+              w = w_get<PERSIST>(s, (long long)(r0 + r) * s.ldc + c);
             } else {
               w = staged_lookup<ST>(s_desc[r], ld_st<PERSIST>(s.sol_out + c));
             }

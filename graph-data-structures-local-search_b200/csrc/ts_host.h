@@ -65,6 +65,7 @@ struct ts_graph {
   int64_t entries = 0;
   int64_t max_wdeg = 0;
   bool neg_w = false;  // some edge weight is negative
+  int64_t max_abs_w = 0;  // largest |w| of an entry
   int64_t wpr = 0;
   int64_t hash_slots = 0;
   tsb::DevBuf rowptr, adj, bits, hoff, hkey, hval, rev;
@@ -101,8 +102,25 @@ namespace tsb {
 void mdp_random_set(int32_t n, int32_t m, uint32_t seed, std::vector<int32_t>& ids);
 void maxbs_random_part(std::mt19937& rng, int32_t n, std::vector<uint8_t>& side0);
 void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out);
-// Dynamic shared memory for staging R rows of a lookup structure.
+// Dynamic shared memory for staging R rows of a lookup structure (the pass
+// with per-row registers).
 int32_t staging_bytes(const ts_graph* g, int R);
+
+// Tile shape of a solve, shared by the plain, batched and served forms: rows
+// per tile, whether the fast pass runs (32-bit keys) and its index capacity,
+// the CSR adjacency mask, column chunks (a multiple of one pass of the CTA, at
+// least `min_tiles` tiles where the columns allow) and the dynamic shared
+// memory one tile needs.
+struct TileGeom {
+  int32_t rows = 0, n_row_blocks = 0, chunk_cols = 0, n_chunks = 0;
+  int32_t fast = 0, fast_ecap = 0, adj_mask = 0, stage_bytes = 0;
+  size_t smem = 16;
+};
+TileGeom tile_geometry(const ts_graph* g, int32_t problem, int32_t m, bool wide, int64_t min_tiles,
+                       int32_t pass);
+// WSwap: the matrix holds 16-bit weights when every |w| fits (the patch of a
+// move clears and sets elements, so an element only ever holds one weight).
+bool wswap_w16(const ts_graph* g);
 // Opts kernel `fn` in to `smem` bytes of dynamic shared memory on the current
 // device.  The limit only grows (under a lock), so a launch planned earlier
 // with a larger size stays valid when a smaller one is planned later.

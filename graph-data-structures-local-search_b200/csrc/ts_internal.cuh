@@ -32,6 +32,7 @@ enum : int32_t {
   E_BAD_INDEX = 4,
   E_BAD_EDGE = 8,
   E_HASH_FULL = 16,
+  E_BULK_TIMEOUT = 32,  // a bulk copy into shared memory did not complete in time
 };
 
 struct DevGraph {
@@ -94,6 +95,15 @@ struct DevSolver {
   // MaxBS only when a weight is negative (with w >= 0 the w-free gain of an
   // adjacent pair under-estimates it and cannot win).
   int32_t adj_mask;
+  // Tile geometry: inside positions per tile; the fast pass (32-bit keys:
+  // one structure query per column for all the tile's rows) and its index
+  // capacity in row entries.
+  int32_t tile_rows;
+  int32_t fast;
+  int32_t fast_ecap;
+  // WSwap: 1 when the matrix holds 16-bit weights (every |w| <= 32767), read
+  // through W as int16_t; 0: 32-bit.
+  int32_t w16;
   int64_t P;
   int32_t* sol_in;
   int32_t* sol_out;
@@ -117,14 +127,16 @@ struct DevSolver {
 // Hash structure: one open-addressing table per vertex, keyed by the
 // neighbour id.  The reference keeps one global table at load <= 0.6 with a
 // MurmurHash3 finaliser (GPU-MDP-Hash.cu:151-158,430-440); here the per-vertex
-// tables trade HBM for short probes: capacity = power of two >= 4*degree
-// (load <= 0.25, at least 8 slots), split into 4-slot buckets read with one
+// tables keep every probe short: capacity = power of two >= 2*degree
+// (load <= 0.5, at least 8 slots), split into 4-slot buckets read with one
 // 16-byte load; the home bucket is a Fibonacci multiplicative hash and a full
 // bucket spills to the next one.  A lookup that meets an empty slot in a
-// bucket without the key is a miss (no deletions ever happen).
+// bucket without the key is a miss (no deletions ever happen).  The sweep
+// reads a tile's tables once to build its own shared-memory index, so the
+// table size is also the structure's HBM traffic per row.
 __host__ __device__ __forceinline__ int64_t hash_capacity(int64_t deg) {
   int64_t cap = 8;
-  while (cap < 4 * deg) cap <<= 1;
+  while (cap < 2 * deg) cap <<= 1;
   return cap;
 }
 __host__ __device__ __forceinline__ uint32_t hash_gshift(int64_t cap) {  // 32 - log2(cap / 4)

@@ -20,6 +20,7 @@ STRUCT_CSR, STRUCT_HASH, STRUCT_WSWAP, STRUCT_CSR_BITSET, STRUCT_CSR_BB, STRUCT_
 STRUCT_NAMES = ["csr", "hash", "wswap", "csr-bitset", "csr-bb", "csr-bitset-bb"]
 PROBLEM_MDP, PROBLEM_MAXBS = 0, 1
 TENURE_REF, TENURE_FIXED = 0, 1
+PASS_AUTO, PASS_TILE, PASS_ROWS = 0, 1, 2
 
 # Every symbol include/ts_b200.h declares.
 EXPORTS = [
@@ -64,7 +65,7 @@ class Params(ctypes.Structure):
         ("problem", ctypes.c_int32), ("m", ctypes.c_int32), ("max_iter", ctypes.c_int64),
         ("tenure_policy", ctypes.c_int32), ("tenure", ctypes.c_int32), ("maxt", ctypes.c_int32),
         ("piter", ctypes.c_int32), ("gamma", ctypes.c_int32), ("seed", ctypes.c_uint32),
-        ("trace", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("trace", ctypes.c_int32), ("pass_", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 

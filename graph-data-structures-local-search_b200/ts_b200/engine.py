@@ -121,7 +121,8 @@ class Solver:
 
     def __init__(self, graph: Graph, problem: int, *, m: int = 0, max_iter: int = 50000,
                  tenure_policy: int = C.TENURE_REF, tenure: int = 15, maxt: int = 200,
-                 piter: int = 500, gamma: int = 150, seed: int = 1, trace: bool = False):
+                 piter: int = 500, gamma: int = 150, seed: int = 1, trace: bool = False,
+                 sweep: int = C.PASS_AUTO):
         self.graph = graph
         p = default_params(problem)
         p.m = m
@@ -133,6 +134,7 @@ class Solver:
         p.gamma = gamma
         p.seed = seed & 0xFFFFFFFF
         p.trace = int(trace)
+        p.pass_ = int(sweep)
         self.params = p
         self.problem = problem
         h = ctypes.c_void_p()
@@ -278,6 +280,7 @@ class BatchJobSpec:
     seed: int = 1
     initial: np.ndarray | None = None
     cluster: int = 0  # CTAs per solve: 0 auto, 1, 2, 4 or 8
+    sweep: int = C.PASS_AUTO  # ts_pass
 
 
 class Batch:
@@ -303,6 +306,7 @@ class Batch:
             p.piter = j.piter
             p.gamma = j.gamma
             p.seed = j.seed & 0xFFFFFFFF
+            p.pass_ = int(j.sweep)
             arr[q].graph = j.graph.handle.value
             arr[q].params = p
             init = None if j.initial is None else np.ascontiguousarray(j.initial, dtype=np.int32)

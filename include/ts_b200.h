@@ -65,6 +65,15 @@ typedef enum ts_problem { TS_PROBLEM_MDP = 0, TS_PROBLEM_MAXBS = 1 } ts_problem;
  * C2=round(0.7*tenure); MaxBS tt=tenure. */
 typedef enum ts_tenure { TS_TENURE_REF = 0, TS_TENURE_FIXED = 1 } ts_tenure;
 
+/* How an iteration sweeps the swap pairs; every choice gives the same moves.
+ * TS_PASS_TILE: a tile of 32 inside positions builds a shared-memory index of
+ *   its rows' adjacency from the structure and queries each outside position
+ *   once for all 32 rows (32-bit keys only; 64-bit keys use TS_PASS_ROWS).
+ * TS_PASS_ROWS: a few rows per tile, each pair looked up in its row's staged
+ *   structure (fewer, cheaper tiles: small instances).
+ * TS_PASS_AUTO: TILE from 2^22 swap pairs per iteration up, else ROWS. */
+typedef enum ts_pass { TS_PASS_AUTO = 0, TS_PASS_TILE = 1, TS_PASS_ROWS = 2 } ts_pass;
+
 typedef struct ts_graph ts_graph;
 typedef struct ts_solver ts_solver;
 
@@ -104,7 +113,8 @@ typedef struct ts_params {
   int32_t gamma;          /* MaxBS perturbation strength (default 150) */
   uint32_t seed;          /* random start + perturbation stream */
   int32_t trace;          /* 1: keep a per-iteration trace on the device */
-  int32_t reserved[7];    /* zero */
+  int32_t pass;           /* pair sweep (ts_pass; no counterpart in the reference): 0 = by size */
+  int32_t reserved[6];    /* zero */
 } ts_params;
 
 typedef struct ts_result {

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def plain(spec):
     s = T.Solver(spec.graph, spec.problem, m=spec.m, max_iter=spec.max_iter,
                  tenure_policy=spec.tenure_policy, tenure=spec.tenure, maxt=spec.maxt,
-                 piter=spec.piter, gamma=spec.gamma, seed=spec.seed)
+                 piter=spec.piter, gamma=spec.gamma, seed=spec.seed, sweep=spec.sweep)
     try:
         s.init(spec.initial)
         s.step(spec.max_iter)
@@ -40,7 +40,7 @@ def graph(n, u, v, w, kind, problem):
     return T.Graph(n, u, v, w, kind, drop_self_loops=problem == T.PROBLEM_MDP)
 
 
-def mixed_specs(kind):
+def mixed_specs(kind, sweep=T.PASS_AUTO):
     """MDP and MaxBS solves on small graphs, seeded and explicit starts."""
     specs, graphs = [], []
     for seed in (1, 2):
@@ -76,12 +76,15 @@ def mixed_specs(kind):
     part[np.arange(0, 500, 2)] = 0
     specs.append(T.BatchJobSpec(g, T.PROBLEM_MAXBS, max_iter=200, tenure_policy=T.TENURE_FIXED,
                                 tenure=10, piter=50, gamma=40, seed=12, initial=part))
+    for sp in specs:
+        sp.sweep = sweep
     return specs, graphs
 
 
+@pytest.mark.parametrize("sweep", [T.PASS_TILE, T.PASS_ROWS], ids=["tile", "rows"])
 @pytest.mark.parametrize("kind", T.STRUCT_NAMES)
-def test_batch_matches_plain(gpu, kind):
-    specs, graphs = mixed_specs(kind)
+def test_batch_matches_plain(gpu, kind, sweep):
+    specs, graphs = mixed_specs(kind, sweep)
     got = T.batch_solve(specs)
     for q, s in enumerate(specs):
         assert_same(got[q], plain(s), f"{kind} job {q}")
@@ -108,17 +111,19 @@ def test_batch_all_structures_in_one_launch_and_replay(gpu):
         g.close()
 
 
-@pytest.mark.parametrize("kind", ["csr", "wswap", "csr-bitset-bb", "hash"])
-def test_cluster_sizes_agree_with_oracle(gpu, kind):
+@pytest.mark.parametrize("sweep", [T.PASS_TILE, T.PASS_ROWS], ids=["tile", "rows"])
+@pytest.mark.parametrize("kind", ["csr", "wswap", "csr-bitset-bb", "hash", "csr-bb", "csr-bitset"])
+def test_cluster_sizes_agree_with_oracle(gpu, kind, sweep):
     c = T.gen.config1()
     n, m = c["n"], c["m"]
     g = graph(n, c["u"], c["v"], c["w"], kind, T.PROBLEM_MDP)
     specs = [T.BatchJobSpec(g, T.PROBLEM_MDP, m=m, max_iter=200, tenure_policy=T.TENURE_FIXED,
-                            tenure=20, seed=1, cluster=cs) for cs in (1, 2, 4, 8)]
+                            tenure=20, seed=1, cluster=cs, sweep=sweep) for cs in (1, 2, 4, 8)]
     u, v, w = node_weight_graph(1500, 10.0, 7)
     gb = graph(1500, u, v, w, kind, T.PROBLEM_MAXBS)
     specs += [T.BatchJobSpec(gb, T.PROBLEM_MAXBS, max_iter=300, tenure_policy=T.TENURE_FIXED,
-                             tenure=25, piter=60, gamma=50, seed=5, cluster=cs) for cs in (1, 2, 4, 8)]
+                             tenure=25, piter=60, gamma=50, seed=5, cluster=cs, sweep=sweep)
+              for cs in (1, 2, 4, 8)]
     got = T.batch_solve(specs)
     og = O.Graph(n, c["u"], c["v"], c["w"], drop_self_loops=True)
     om = O.run(og, O.MDP, m=m, max_iter=200, tenure_policy=T.TENURE_FIXED, tenure=20, seed=1, threads=0)

@@ -10,7 +10,7 @@ oracle (one oracle run per configuration: the trajectory does not depend on
 the structure):
 
 * config 1 -- MDP, Erdos-Renyi n = 2,000, mean degree 20, m = 200, tenure 20,
-  all 10,000 iterations;
+  all 10,000 iterations, with each of the two pair sweeps;
 * config 3 -- MDP, Chung-Lu n = 200,000 (exponent 2.3, mean degree 50, max
   5,000), m = 2,000, tenure 100, all 500 iterations;
 * config 2 -- Max Bisection, conflict graph n = 100,000 (2.5e9 pairs per
@@ -35,11 +35,12 @@ pytestmark = pytest.mark.gpu
 STRUCTS = T.STRUCT_NAMES
 
 
-def gpu_run(problem, kind, wl, *, m, iters, tenure, piter=500, gamma=150, seed=1, initial=None):
+def gpu_run(problem, kind, wl, *, m, iters, tenure, piter=500, gamma=150, seed=1, initial=None,
+            sweep=T.PASS_AUTO):
     drop = problem == T.PROBLEM_MDP
     g = T.Graph(wl["n"], wl["u"], wl["v"], wl["w"], kind, drop_self_loops=drop)
     s = T.Solver(g, problem, m=m, max_iter=iters, tenure_policy=T.TENURE_FIXED, tenure=tenure,
-                 piter=piter, gamma=gamma, seed=seed, trace=True)
+                 piter=piter, gamma=gamma, seed=seed, trace=True, sweep=sweep)
     try:
         s.init(initial)
         done = s.step(iters)
@@ -84,10 +85,11 @@ def c1():
     return wl, ores
 
 
+@pytest.mark.parametrize("sweep", [T.PASS_TILE, T.PASS_ROWS], ids=["tile", "rows"])
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_config1_full_10000_iterations(gpu, c1, kind):
+def test_config1_full_10000_iterations(gpu, c1, kind, sweep):
     wl, ores = c1
-    got = gpu_run(T.PROBLEM_MDP, kind, wl, m=wl["m"], iters=10_000, tenure=20)
+    got = gpu_run(T.PROBLEM_MDP, kind, wl, m=wl["m"], iters=10_000, tenure=20, sweep=sweep)
     assert_same(kind, T.PROBLEM_MDP, wl["n"], got, ores)
 
 

@@ -2,7 +2,9 @@
 
 Every case compares, per iteration, the chosen flat move index, its key, the
 objective bookkeeping (cur/best) and the tenures; then the final positions,
-tabu list and contributions, and the best solution.
+tabu list and contributions, and the best solution.  The cases run both pair
+sweeps (``sweep``): the tile pass (one structure query per column for a tile
+of 32 rows) and the per-row pass, which the library picks by instance size.
 """
 import numpy as np
 import pytest
@@ -13,6 +15,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 STRUCTS = T.STRUCT_NAMES
+SWEEPS = pytest.mark.parametrize("sweep", [T.PASS_TILE, T.PASS_ROWS], ids=["tile", "rows"])
 
 
 def rand_graph(n, p, seed, wlo=1, whi=1000, dup=False, selfloops=False):
@@ -39,7 +42,7 @@ def node_weight_graph(n, avg_deg, seed):
 
 
 def compare_run(problem, kind, n, u, v, w, *, m=0, iters, tenure_policy, tenure=0, maxt=200,
-                piter=500, gamma=150, seed=1, initial=None, step_chunks=(None,)):
+                piter=500, gamma=150, seed=1, initial=None, step_chunks=(None,), sweep=T.PASS_AUTO):
     drop = problem == T.PROBLEM_MDP
     og = O.Graph(n, u, v, w, drop_self_loops=drop)
     ores = O.run(og, O.MDP if problem == T.PROBLEM_MDP else O.MAXBS, m=m, max_iter=iters,
@@ -47,7 +50,7 @@ def compare_run(problem, kind, n, u, v, w, *, m=0, iters, tenure_policy, tenure=
                  seed=seed, initial=initial, threads=0)
     g = T.Graph(n, u, v, w, kind, drop_self_loops=drop)
     s = T.Solver(g, problem, m=m, max_iter=iters, tenure_policy=tenure_policy, tenure=tenure,
-                 maxt=maxt, piter=piter, gamma=gamma, seed=seed, trace=True)
+                 maxt=maxt, piter=piter, gamma=gamma, seed=seed, trace=True, sweep=sweep)
     try:
         s.init(initial)
         done = 0
@@ -86,108 +89,118 @@ def compare_run(problem, kind, n, u, v, w, *, m=0, iters, tenure_policy, tenure=
     return ores
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
 @pytest.mark.parametrize("seed", [1, 2, 3])
-def test_mdp_small_ref_tenure(gpu, kind, seed):
+def test_mdp_small_ref_tenure(gpu, kind, seed, sweep):
     n, m = 60, 10
     u, v, w = rand_graph(n, 0.3, seed, whi=50)
     compare_run(T.PROBLEM_MDP, kind, n, u, v, w, m=m, iters=400, tenure_policy=T.TENURE_REF,
-                seed=seed)
+                seed=seed, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_mdp_config1_shape(gpu, kind):
+def test_mdp_config1_shape(gpu, kind, sweep):
     # ER n=2000, mean degree 20, m=200, fixed tenure 20 (C2=14), reference random start.
     c = T.gen.config1()
     compare_run(T.PROBLEM_MDP, kind, c["n"], c["u"], c["v"], c["w"], m=c["m"], iters=300,
-                tenure_policy=T.TENURE_FIXED, tenure=20, seed=1)
+                tenure_policy=T.TENURE_FIXED, tenure=20, seed=1, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_mdp_all_tabu_break(gpu, kind):
+def test_mdp_all_tabu_break(gpu, kind, sweep):
     n, m = 8, 4
     a, b = np.triu_indices(n, 1)
     w = np.full(len(a), 7, np.int32)
     o = compare_run(T.PROBLEM_MDP, kind, n, a.astype(np.int32), b.astype(np.int32), w, m=m,
                     iters=100, tenure_policy=T.TENURE_FIXED, tenure=50,
-                    initial=np.array([0, 1, 2, 3], np.int32))
+                    initial=np.array([0, 1, 2, 3], np.int32), sweep=sweep)
     assert o.stopped
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_mdp_duplicates_ties_and_extremes(gpu, kind):
+def test_mdp_duplicates_ties_and_extremes(gpu, kind, sweep):
     # duplicated edges (contributions sum, lookup = first entry), uniform weights (ties)
     n = 50
     u, v, w = rand_graph(n, 0.25, 9, dup=True)
     compare_run(T.PROBLEM_MDP, kind, n, u, v, w, m=7, iters=200, tenure_policy=T.TENURE_FIXED,
-                tenure=6, seed=4)
+                tenure=6, seed=4, sweep=sweep)
     u, v, _ = rand_graph(n, 0.3, 10)
     compare_run(T.PROBLEM_MDP, kind, n, u, v, np.full(len(u), 3, np.int32), m=9, iters=200,
-                tenure_policy=T.TENURE_REF, seed=5)
+                tenure_policy=T.TENURE_REF, seed=5, sweep=sweep)
     # m = 1 and m = n-1
     compare_run(T.PROBLEM_MDP, kind, n, u, v, np.full(len(u), 3, np.int32), m=1, iters=50,
-                tenure_policy=T.TENURE_FIXED, tenure=2, seed=6)
+                tenure_policy=T.TENURE_FIXED, tenure=2, seed=6, sweep=sweep)
     compare_run(T.PROBLEM_MDP, kind, n, u, v, np.full(len(u), 3, np.int32), m=n - 1, iters=50,
-                tenure_policy=T.TENURE_FIXED, tenure=2, seed=7)
+                tenure_policy=T.TENURE_FIXED, tenure=2, seed=7, sweep=sweep)
     # no edges at all
     e = np.zeros(0, np.int32)
     compare_run(T.PROBLEM_MDP, kind, n, e, e, e, m=5, iters=30, tenure_policy=T.TENURE_FIXED,
-                tenure=3, seed=8)
+                tenure=3, seed=8, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
 @pytest.mark.parametrize("seed", [1, 2])
-def test_maxbs_small_penalised_and_perturbed(gpu, kind, seed):
+def test_maxbs_small_penalised_and_perturbed(gpu, kind, seed, sweep):
     n = 41
     u, v, w = rand_graph(n, 0.25, 20 + seed, whi=60)
     compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=300, tenure_policy=T.TENURE_FIXED,
-                tenure=30, piter=25, gamma=12, seed=seed)
+                tenure=30, piter=25, gamma=12, seed=seed, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_maxbs_ref_tenure_perturbation(gpu, kind):
+def test_maxbs_ref_tenure_perturbation(gpu, kind, sweep):
     n = 500
     u, v, w = node_weight_graph(n, 12.0, 3)
     o = compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=600, tenure_policy=T.TENURE_REF,
-                    maxt=40, piter=40, gamma=30, seed=3)
+                    maxt=40, piter=40, gamma=30, seed=3, sweep=sweep)
     assert (o.trace["kind"] == O.REC_PERTURB).any()
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_maxbs_odd_n_selfloops_and_steps(gpu, kind):
+def test_maxbs_odd_n_selfloops_and_steps(gpu, kind, sweep):
     n = 201
     u, v, w = rand_graph(n, 0.05, 31, selfloops=True)
     compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=250, tenure_policy=T.TENURE_FIXED,
-                tenure=7, piter=30, gamma=20, seed=9, step_chunks=(1, 17, 100))
+                tenure=7, piter=30, gamma=20, seed=9, step_chunks=(1, 17, 100), sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_maxbs_explicit_partition(gpu, kind):
+def test_maxbs_explicit_partition(gpu, kind, sweep):
     n = 300
     u, v, w = node_weight_graph(n, 9.0, 4)
     part = np.ones(n, np.int32)
     part[np.arange(0, n, 2)[: n // 2]] = 0
     compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=200, tenure_policy=T.TENURE_FIXED,
-                tenure=10, piter=50, gamma=40, seed=12, initial=part)
+                tenure=10, piter=50, gamma=40, seed=12, initial=part, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
 @pytest.mark.parametrize("n,p", [(120, 0.2), (2600, 0.01)])
-def test_maxbs_negative_weights(gpu, kind, n, p):
+def test_maxbs_negative_weights(gpu, kind, n, p, sweep):
     # Weights of both signs (the instance readers accept negative fixed-point
     # weights): no sweep may assume w >= 0 for adjacent pairs.  n = 2600 puts
     # several 1024-column passes in a row.
     u, v, w = rand_graph(n, p, 41 + n, wlo=-1000, whi=1000)
     compare_run(T.PROBLEM_MAXBS, kind, n, u, v, w, iters=200, tenure_policy=T.TENURE_FIXED,
-                tenure=15, piter=40, gamma=20, seed=5)
+                tenure=15, piter=40, gamma=20, seed=5, sweep=sweep)
 
 
+@SWEEPS
 @pytest.mark.parametrize("kind", STRUCTS)
-def test_mdp_negative_weights(gpu, kind):
+def test_mdp_negative_weights(gpu, kind, sweep):
     n, m = 300, 40
     u, v, w = rand_graph(n, 0.1, 77, wlo=-500, whi=500)
     compare_run(T.PROBLEM_MDP, kind, n, u, v, w, m=m, iters=300, tenure_policy=T.TENURE_FIXED,
-                tenure=10, seed=4)
+                tenure=10, seed=4, sweep=sweep)
 
 
 def test_lookup_interface_all_structures(gpu):
