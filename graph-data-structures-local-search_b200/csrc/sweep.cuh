@@ -1230,12 +1230,13 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
 // Plain form: one launch = one iteration; CTA b evaluates tile b, the last
 // CTA to finish reduces the records and applies the move.
 // Minimum resident CTAs per SM the plain kernel is compiled for (0: left to
-// the compiler).  MDP WSwap with 32-bit keys is held to 64 registers so four
-// CTAs share an SM: the matrix stream is bound by loads in flight, and the
-// fourth CTA moves an n = 200,000, m = 2,000 sweep from 4.3 to 4.9 TB/s
-// (a few bytes of spills, outside the sweep loop, cost less than the lost CTA).
-template <int PROB, int ST, class KeyT> struct IterMinBlocks { static constexpr int v = 0; };
-template <> struct IterMinBlocks<P_MDP, S_WSWAP, int32_t> { static constexpr int v = 4; };
+// the compiler).  The 512-thread index structures are held to two CTAs per SM
+// (at most 64 registers): their sweep hides latency with warps.  WSwap is
+// left to the compiler: holding it to 64-80 registers spilled its 16 rows of
+// packed matrix loads.
+template <int PROB, int ST, class KeyT> struct IterMinBlocks {
+  static constexpr int v = (ST == S_CSR || ST == S_WSWAP) ? 0 : 2;
+};
 
 template <int PROB, int ST, class KeyT>
 __global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT>::v))
