@@ -273,7 +273,8 @@ def run_ours(args):
     for k in kinds:
         g = T.Graph(n, u, v, w, k, drop_self_loops=mdp, stream=stream.cuda_stream)
         s = T.Solver(g, problem, m=m if mdp else 0, max_iter=10**9, tenure_policy=T.TENURE_FIXED,
-                     tenure=wl["tenure"], piter=500, gamma=150, seed=seed)
+                     tenure=wl["tenure"], piter=500, gamma=150, seed=seed,
+                     sweep={"auto": T.PASS_AUTO, "tile": T.PASS_TILE, "rows": T.PASS_ROWS}[args.sweep])
         s.init(None)
         graphs[k], solvers[k] = g, s
     total = args.warmup + args.steps
@@ -667,12 +668,13 @@ def run_batched(T, torch, dev, args):
         mdp = inst["problem"] == "mdp"
         prob = T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS
         kind, _ = table.pick(prob, inst["n"])
+        sweep = table.pick_sweep(prob, inst["n"])
         g = T.Graph(inst["n"], u, v, w, kind, drop_self_loops=mdp)
         graphs.append(g)
         for sd in inst["seeds"]:
             specs.append(T.BatchJobSpec(g, prob, m=inst["m"] if mdp else 0, max_iter=inst["iters"],
                                         tenure_policy=T.TENURE_FIXED, tenure=20 if mdp else 50,
-                                        piter=500, gamma=150, seed=sd, cluster=0))
+                                        piter=500, gamma=150, seed=sd, cluster=0, sweep=sweep))
     b = T.Batch(specs, stream=stream.cuda_stream)
     b.launch()
     b.sync()
@@ -703,7 +705,7 @@ def run_batched(T, torch, dev, args):
         sp = specs[q]
         t0 = time.time()
         sv = T.Solver(sp.graph, sp.problem, m=sp.m, max_iter=sp.max_iter, tenure_policy=sp.tenure_policy,
-                      tenure=sp.tenure, piter=sp.piter, gamma=sp.gamma, seed=sp.seed)
+                      tenure=sp.tenure, piter=sp.piter, gamma=sp.gamma, seed=sp.seed)  # plain: its own auto sweep
         sv.init(None)
         sv.step(sp.max_iter)
         r = sv.result()
@@ -732,6 +734,7 @@ def run_batched(T, torch, dev, args):
         "identical_to_plain": bool(identical),
         "groups": info.groups, "slots": info.slots, "slot_bytes": info.slot_bytes,
         "autotune": table.as_dict(), "autotune_s": t_tune,
+        "autotune_unavailable": [t for t in table.trials if "unavailable" in t],
     }
 
 
@@ -846,6 +849,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="config2/config3 at another size (profiling cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, CPU-baseline and batched legs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (config 4) leg")
+    ap.add_argument("--sweep", choices=["auto", "tile", "rows"], default="auto",
+                    help="pair sweep of the main leg's solvers (ts_pass; auto picks by size)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the config-1/config-3 legs and the reference CUDA build's timing")
     ap.add_argument("--c4-instances", type=int, default=40, help="batched leg: instances of config 4")

@@ -104,7 +104,7 @@ __device__ DevSolver<KeyT> slot_solver(const BatchJobDev& J, const SlotPool<KeyT
 }
 
 template <int PROB, int ST, class KeyT>
-__global__ void __launch_bounds__(Tpb<ST>::v)
+__global__ void __launch_bounds__((TpbOf<ST, true>::v))
 batch_kernel(const BatchJobDev* __restrict__ jobs, int njobs, BatchResultDev* __restrict__ out,
              int32_t* __restrict__ best_out, const SlotPool<KeyT> pool, unsigned int* next_job) {
   cg::cluster_group cl = cg::this_cluster();
@@ -241,8 +241,7 @@ template <int PROB, int ST, class KeyT>
 ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_bytes,
                      int32_t max_slots, int sms) {
   constexpr int R = Rows<ST>::R;
-  constexpr int TPB = Tpb<ST>::v;
-  const int pc = pass_cols_of(ST);
+  constexpr int TPB = TpbOf<ST, true>::v;
   const int cs = G.cluster;
   long long max_m = 1, max_n = 1, max_ldc = 4, max_entries = 1, max_w = 1, log_cap = 1;
   size_t smem = 16;
@@ -253,7 +252,7 @@ ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_b
     const long long ldc = (delta + 3) & ~3;
     // tiles as in the plain solver, full row width where it fits; a cluster
     // gets at least one tile per CTA
-    const TileGeom tg = tile_geometry(H.g, PROB, H.m, sizeof(KeyT) == 8, cs, H.p.pass);
+    const TileGeom tg = tile_geometry(H.g, PROB, H.m, sizeof(KeyT) == 8, cs, H.p.pass, true);
     J.n_row_blocks = tg.n_row_blocks;
     J.tile_rows = tg.rows;
     J.fast = tg.fast;
@@ -290,7 +289,15 @@ ts_status plan_group(Group& G, std::vector<BatchJobDev>& table, int64_t budget_b
   int resident = 0;
   TS_CUDA(cudaOccupancyMaxActiveClusters(&resident, kern, &cfg));
   if (resident < 1) {
-    set_error("ts_batch_create: a cluster of " + std::to_string(cs) + " CTAs does not fit on the device");
+    cudaFuncAttributes fa;
+    std::string why;
+    if (cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kern)) == cudaSuccess)
+      why = " (" + std::to_string(TPB) + " threads x " + std::to_string(fa.numRegs) + " registers, " +
+            std::to_string(fa.sharedSizeBytes) + " B static + " + std::to_string(smem) +
+            " B dynamic shared memory per CTA)";
+    else
+      cudaGetLastError();
+    set_error("ts_batch_create: a cluster of " + std::to_string(cs) + " CTAs does not fit on the device" + why);
     return TS_ERR_UNSUPPORTED;
   }
   // slices padded to 256 B; strides in elements of each array

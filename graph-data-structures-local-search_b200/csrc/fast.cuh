@@ -40,6 +40,8 @@ namespace tsb {
 
 constexpr int kFastRows = 32;  // rows per tile: one bit each in a 32-bit mask
 constexpr int kTabuQueue = 1024;  // tabu columns a tile evaluates warp-wide (more: per lane)
+constexpr int kTrack = 4;          // high-degree rows whose own best free column the sweep tracks
+constexpr int32_t kTrackDeg = 256; // ... from this degree up
 constexpr int kTopK = 2;       // column candidates kept per thread and per tile (the
                                // per-thread insertion below is written out for two)
 
@@ -174,6 +176,10 @@ struct FastSh {
   unsigned long long red[kMaxTPB / 32];
   unsigned long long mbar;
   int32_t qn;
+  int32_t trk[kTrack];          // tracked rows of the group (see kTrack)
+  int32_t ntrk;
+  uint32_t trk_mask;
+  unsigned long long trkbest[kTrack];  // packed (contribution, column) per tracked row
   int32_t tqn;                  // tabu columns queued for the warp-wide evaluation
   int32_t tq[kTabuQueue];
   int32_t ntop;
@@ -685,6 +691,29 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
       sh.done_rows |= grp;
       sh.qn = 0;
       sh.tqn = 0;
+      // Hub rows are adjacent to every top column (hubs are adjacent to each
+      // other), so the shared top-2 rarely serves them: the sweep tracks the
+      // best free column of up to kTrack of the group's highest-degree rows.
+      // (CSR without the adjacency mask needs none: its w-free gains only
+      // under-estimate adjacent pairs.)
+      int32_t nt = 0;
+      uint32_t tm = 0u;
+      if (ST != S_CSR || masked_csr) {
+        for (int t = 0; t < kTrack; t++) {
+          int best_r = -1;
+          for (int r = 0; r < nr; r++)
+            if (((grp >> r) & 1u) && !((tm >> r) & 1u) && sh.rdeg[r] >= kTrackDeg &&
+                (best_r < 0 || sh.rdeg[r] > sh.rdeg[best_r]))
+              best_r = r;
+          if (best_r < 0) break;
+          tm |= 1u << best_r;
+          sh.trk[nt] = best_r;
+          sh.trkbest[nt] = 0ull;
+          nt++;
+        }
+      }
+      sh.ntrk = nt;
+      sh.trk_mask = tm;
       sh.rescan = 0u;
     }
     __syncthreads();
@@ -785,6 +814,11 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
 #pragma unroll
     for (int k = 0; k < kTopK; k++) { tcv[k] = INT32_MIN; tc[k] = INT32_MAX; tmk[k] = 0u; }
     int32_t* Q = ix.queue();
+    const int ntrk = sh.ntrk;
+    int trk[kTrack];
+    unsigned long long hb[kTrack];
+#pragma unroll
+    for (int h = 0; h < kTrack; h++) { trk[h] = sh.trk[h]; hb[h] = 0ull; }
     // one pass of loads in flight ahead of the pass being evaluated
     const int32_t it32 = iter > (long long)INT32_MAX ? INT32_MAX : (int32_t)iter;  // tabu stamps are int32
     int32_t cb = c0 + tid * kColsPerLane;
@@ -842,6 +876,19 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
         for (int q = 0; q < 4; q++)
           if (adj[q] && !tb[q]) Q[atomicAdd(&sh.qn, 1)] = cb + q;
       }
+      if (ntrk) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (!ok[q] || tb[q]) continue;
+          uint32_t mkq = 0u;
+          if (ST == S_CSR) mkq = s_mask[cb + q - c0];
+          else if (adj[q]) mkq = ix.mask_of(vx[q]);
+          const unsigned long long p = pack_kc(cv[q], cb + q);
+#pragma unroll
+          for (int h = 0; h < kTrack; h++)
+            if (h < ntrk && !((mkq >> trk[h]) & 1u)) hb[h] = p > hb[h] ? p : hb[h];
+        }
+      }
       if (m4 > tcv[1]) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -882,6 +929,12 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
         const int32_t x = pair_gain<PROB, int32_t>(sh.rv[r], cvv, w);
         if (x > D) atomicMax(&sh.best[r], pack_kc(x, c));
       }
+    }
+
+    // ---------------- tracked rows: their best free column, block-wide
+    for (int h = 0; h < ntrk; h++) {
+      const unsigned long long m = warp_max_u64(hb[h]);
+      if (lane == 0 && m) atomicMax(&sh.trkbest[h], m);
     }
 
     // ---------------- exact pairs of the adjacent columns
@@ -931,8 +984,15 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
       if (lane == 0) sh.ntop = cnt;
     }
     __syncthreads();
-    // each row: its first top column it is not adjacent to (w-free gain)
-    if (tid < kFastRows && ((grp >> tid) & 1u)) {
+    // each row: its first top column it is not adjacent to (w-free gain);
+    // a tracked row has its own best free column
+    if (tid < sh.ntrk && sh.trkbest[tid]) {
+      const int r = sh.trk[tid];
+      const unsigned long long p = sh.trkbest[tid];
+      const int32_t x = pair_gain<PROB, int32_t>(sh.rv[r], unpack_key(p), 0);
+      atomicMax(&sh.best[r], pack_kc(x, unpack_col(p)));
+    }
+    if (tid < kFastRows && ((grp >> tid) & 1u) && !((sh.trk_mask >> tid) & 1u)) {
       const int r = tid;
       bool found = false;
       for (int k = 0; k < sh.ntop && !found; k++) {

@@ -53,7 +53,7 @@ struct ServeJobDev {
 
 // One cluster per job; the job runs until stop_at, its end or max_iter.
 template <int PROB, int ST, class KeyT>
-__global__ void __launch_bounds__(Tpb<ST>::v)
+__global__ void __launch_bounds__((TpbOf<ST, true>::v))
 serve_kernel(const ServeJobDev<KeyT>* __restrict__ jobs) {
   cg::cluster_group cl = cg::this_cluster();
   const unsigned rank = cl.block_rank(), cs = cl.num_blocks();
@@ -87,7 +87,7 @@ cudaError_t launch_serve(cudaStream_t st, const void* jobs, int njobs, int cs, s
   a[0].val.clusterDim.z = 1;
   cudaLaunchConfig_t c = {};
   c.gridDim = dim3((unsigned)(njobs * cs));
-  c.blockDim = dim3(Tpb<ST>::v);
+  c.blockDim = dim3(TpbOf<ST, true>::v);
   c.dynamicSmemBytes = smem;
   c.stream = st;
   c.attrs = a;
@@ -227,7 +227,7 @@ ts_status build_packed(Req& r, int32_t kind) {
   const int c1s[4] = {15, 30, 60, 120};
   for (int i = 0; i < 4; i++) s.c2_tab[i] = (int32_t)round(0.7 * c1s[i]);
   s.c2_fixed = (int32_t)round(0.7 * r.p.tenure);
-  const TileGeom tg = tile_geometry(r.g, r.p.problem, m, sizeof(KeyT) == 8, r.cs, r.p.pass);
+  const TileGeom tg = tile_geometry(r.g, r.p.problem, m, sizeof(KeyT) == 8, r.cs, r.p.pass, true);
   s.n_row_blocks = tg.n_row_blocks;
   s.tile_rows = tg.rows;
   s.fast = tg.fast;

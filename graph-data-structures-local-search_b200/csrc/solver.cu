@@ -106,7 +106,7 @@ int32_t staging_bytes(const ts_graph* g, int R) {
 bool wswap_w16(const ts_graph* g) { return g->max_abs_w <= 32767; }
 
 TileGeom tile_geometry(const ts_graph* g, int32_t problem, int32_t m, bool wide, int64_t min_tiles,
-                       int32_t pass) {
+                       int32_t pass, bool persist) {
   TileGeom t;
   const int kind = g->kind;
   const int64_t delta = (int64_t)g->n - m;
@@ -124,7 +124,7 @@ TileGeom tile_geometry(const ts_graph* g, int32_t problem, int32_t m, bool wide,
   t.n_row_blocks = (int32_t)((m + t.rows - 1) / t.rows);
   const bool mdp_csr = kind == S_CSR && (problem == P_MDP || g->neg_w);
   t.adj_mask = mdp_csr ? 1 : 0;
-  const int64_t pc = pass_cols_of(kind);
+  const int64_t pc = pass_cols_of(kind, persist);
   const int64_t full = ((delta + pc - 1) / pc) * pc;
   int64_t max_cols = full;
   if (kind == S_WSWAP) max_cols = 8 * pc;
@@ -248,6 +248,9 @@ template <int PROB, int ST, class KeyT>
 cudaError_t launch_iter(const DevGraph& g, const DevSolver<KeyT>& s, int grid, size_t smem,
                         cudaStream_t st, int count) {
   auto fn = iter_kernel<PROB, ST, KeyT>;
+  if constexpr (ST == S_WSWAP) {
+    if (s.w16) fn = iter_kernel<PROB, ST, KeyT, true>;  // compiled for the 16-bit matrix
+  }
   cudaError_t e = allow_dyn_smem(reinterpret_cast<const void*>(fn), smem);
   if (e != cudaSuccess) return e;
   for (int i = 0; i < count; i++) fn<<<grid, Tpb<ST>::v, smem, st>>>(g, s);
@@ -267,25 +270,25 @@ cudaError_t launch_iter_st(int kind, const DevGraph& g, const DevSolver<KeyT>& s
   }
 }
 
-// Resident CTAs per SM of the WSwap iteration kernel.
-int wswap_blocks_per_sm(int problem, bool wide) {
+// Resident CTAs per SM of the WSwap iteration kernel (the one for the
+// matrix's element width).
+template <int PROB, class KeyT>
+int wswap_blocks_for(bool w16) {
   int nb = 0;
-  cudaError_t e;
-  if (problem == P_MDP)
-    e = wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MDP, S_WSWAP, long long>,
-                                                             Tpb<S_WSWAP>::v, 16)
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MDP, S_WSWAP, int32_t>,
-                                                             Tpb<S_WSWAP>::v, 16);
-  else
-    e = wide ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MAXBS, S_WSWAP, long long>,
-                                                             Tpb<S_WSWAP>::v, 16)
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<P_MAXBS, S_WSWAP, int32_t>,
-                                                             Tpb<S_WSWAP>::v, 16);
+  const cudaError_t e =
+      w16 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<PROB, S_WSWAP, KeyT, true>,
+                                                          Tpb<S_WSWAP>::v, 16)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, iter_kernel<PROB, S_WSWAP, KeyT, false>,
+                                                          Tpb<S_WSWAP>::v, 16);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return nb;
+}
+int wswap_blocks_per_sm(int problem, bool wide, bool w16) {
+  if (problem == P_MDP) return wide ? wswap_blocks_for<P_MDP, long long>(w16) : wswap_blocks_for<P_MDP, int32_t>(w16);
+  return wide ? wswap_blocks_for<P_MAXBS, long long>(w16) : wswap_blocks_for<P_MAXBS, int32_t>(w16);
 }
 
 // Column split of a streamed sweep into whole waves: the matrix streams at full
@@ -584,7 +587,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
   // the hardware schedules them.
   const bool staged = g->kind != S_CSR && g->kind != S_WSWAP;
   const int64_t min_grid = staged ? 4 * 148 : (g->kind == S_WSWAP ? 4 * 148 : 2 * 148);
-  const TileGeom tg = tile_geometry(g, p->problem, m, s->wide, min_grid, p->pass);
+  const TileGeom tg = tile_geometry(g, p->problem, m, s->wide, min_grid, p->pass, false);
   s->R = tg.rows;
   s->w16 = g->kind == S_WSWAP && wswap_w16(g) ? 1 : 0;
   s->fast = tg.fast;
@@ -599,7 +602,7 @@ ts_status ts_solver_create(ts_graph* g, const ts_params* p, ts_solver** out) {
       cudaGetLastError();
       sms = 0;  // no wave split: the default chunking stands
     }
-    const int64_t slots = (int64_t)wswap_blocks_per_sm(p->problem, s->wide) * sms;
+    const int64_t slots = (int64_t)wswap_blocks_per_sm(p->problem, s->wide, s->w16 != 0) * sms;
     cols = wave_cols(s->delta, s->n_row_blocks, pc, 8 * pc, 64 * pc, slots, cols);
   }
   s->chunk_cols = (int32_t)cols;

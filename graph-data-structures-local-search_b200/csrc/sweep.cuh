@@ -40,8 +40,16 @@ constexpr int kMaxTPB = 512;
 template <int ST> struct Tpb { static constexpr int v = 512; };
 template <> struct Tpb<S_CSR> { static constexpr int v = 256; };
 template <> struct Tpb<S_WSWAP> { static constexpr int v = 256; };
-__host__ __device__ inline int tpb_of(int st) { return (st == S_CSR || st == S_WSWAP) ? 256 : 512; }
-__host__ __device__ inline int pass_cols_of(int st) { return tpb_of(st) * kColsPerLane; }
+// The persistent kernels (batched and served forms) run 256 threads for every
+// structure: a cluster CTA also holds the solve's init/finish code, and at
+// 512 threads its register budget would not fit an SM.
+template <int ST, bool PERSIST> struct TpbOf { static constexpr int v = PERSIST ? 256 : Tpb<ST>::v; };
+__host__ __device__ inline int tpb_of(int st, bool persist = false) {
+  return (persist || st == S_CSR || st == S_WSWAP) ? 256 : 512;
+}
+__host__ __device__ inline int pass_cols_of(int st, bool persist = false) {
+  return tpb_of(st, persist) * kColsPerLane;
+}
 
 template <int ST> struct Rows { static constexpr int R = 16; };
 template <> struct Rows<S_CSR> { static constexpr int R = 32; };
@@ -625,7 +633,10 @@ __device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mo
 // (PERSIST: state written earlier in the same launch, see ld_st).  floor_key:
 // the best key the caller holds from earlier tiles; a tile whose maximum is
 // below it returns no record.
-template <int PROB, int ST, class KeyT, bool PERSIST>
+// W16K (WSwap, plain kernel only): the kernel is compiled for the 16-bit
+// matrix alone, so its registers are that pass's; otherwise the width is
+// read from the solver at run time.
+template <int PROB, int ST, class KeyT, bool PERSIST, bool W16K = false>
 __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
                           long long D64, int rb, int ch, long long& out_key, long long& out_idx,
                           TailShared& sh, long long floor_key = LLONG_MIN) {
@@ -636,7 +647,7 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
     }
   }
   constexpr int R = Rows<ST>::R;
-  constexpr int TPB = Tpb<ST>::v;
+  constexpr int TPB = TpbOf<ST, PERSIST>::v;
   using Lim = KeyLim<KeyT>;
   const KeyT D = Lim::clampD(D64);
   const int tid = threadIdx.x, lane = tid & 31;
@@ -920,8 +931,8 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         if (ST == S_WSWAP) {
           // Issue every row's W load of this pass before using any: the matrix
           // streams from HBM once per iteration.
-          int4 wv[R];
-          int2 wp[R];
+          int4 wv[W16 ? 1 : R];
+          int2 wp[W16 ? R : 1];
           if constexpr (W16) {
             const int16_t* W16p = reinterpret_cast<const int16_t*>(s.W);
   #pragma unroll
@@ -943,8 +954,10 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
           const bool plain4 = valid[0] && valid[1] && valid[2] && valid[3] && !(ct[0] || ct[1] || ct[2] || ct[3]);
   #pragma unroll
           for (int r = 0; r < R; r++) {
-            if constexpr (W16) wv[r] = unpack_w16(wp[r]);
-            const int32_t w4[4] = {wv[r].x, wv[r].y, wv[r].z, wv[r].w};
+            int4 wr;
+            if constexpr (W16) wr = unpack_w16(wp[r]);
+            else wr = wv[r];
+            const int32_t w4[4] = {wr.x, wr.y, wr.z, wr.w};
             if (plain4) {
               KeyT m = wsw_col_term<PROB, KeyT>(cv[0], w4[0]);
   #pragma unroll
@@ -1123,7 +1136,9 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
         }
       }
     };
-    if constexpr (ST == S_WSWAP) {
+    if constexpr (ST == S_WSWAP && W16K) {
+      sweep_passes(std::true_type{});
+    } else if constexpr (ST == S_WSWAP) {
       if (s.w16) sweep_passes(std::true_type{});
       else sweep_passes(std::false_type{});
     } else {
@@ -1238,7 +1253,7 @@ template <int PROB, int ST, class KeyT> struct IterMinBlocks {
   static constexpr int v = (ST == S_CSR || ST == S_WSWAP) ? 0 : 2;
 };
 
-template <int PROB, int ST, class KeyT>
+template <int PROB, int ST, class KeyT, bool W16K = false>
 __global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT>::v))
 iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   DevState* st = s.st;
@@ -1249,7 +1264,7 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __shared__ TailShared sh;
   __shared__ int32_t s_last;
   long long k, i;
-  tile_eval<PROB, ST, KeyT, false>(g, s, mode, iter, D64, blockIdx.x / s.n_chunks,
+  tile_eval<PROB, ST, KeyT, false, W16K>(g, s, mode, iter, D64, blockIdx.x / s.n_chunks,
                                    blockIdx.x % s.n_chunks, k, i, sh);
   if (threadIdx.x == 0) {
     CtaRec rec;

@@ -106,8 +106,8 @@ void draw_event(std::mt19937& rng, int64_t P, int k, std::vector<long long>& out
 // with per-row registers).
 int32_t staging_bytes(const ts_graph* g, int R);
 
-// Tile shape of a solve, shared by the plain, batched and served forms: rows
-// per tile, whether the fast pass runs (32-bit keys) and its index capacity,
+// Tile shape of a solve, shared by the plain and the persistent (batched,
+// served; `persist`: 256-thread CTAs) forms: rows per tile, whether the fast pass runs (32-bit keys) and its index capacity,
 // the CSR adjacency mask, column chunks (a multiple of one pass of the CTA, at
 // least `min_tiles` tiles where the columns allow) and the dynamic shared
 // memory one tile needs.
@@ -117,7 +117,7 @@ struct TileGeom {
   size_t smem = 16;
 };
 TileGeom tile_geometry(const ts_graph* g, int32_t problem, int32_t m, bool wide, int64_t min_tiles,
-                       int32_t pass);
+                       int32_t pass, bool persist);
 // WSwap: the matrix holds 16-bit weights when every |w| fits (the patch of a
 // move clears and sets elements, so an element only ever holds one weight).
 bool wswap_w16(const ts_graph* g);
