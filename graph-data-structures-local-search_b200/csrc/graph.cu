@@ -36,7 +36,8 @@ ts_status cuda_fail(cudaError_t e, const char* what) {
 }
 
 cudaError_t allow_dyn_smem(const void* fn, size_t smem) {
-  if (smem <= 48 * 1024) return cudaSuccess;
+  // The default limit is 48 KB minus the kernel's static shared memory, so
+  // even a request below 48 KB may need the attribute raised.
   static std::mutex mu;
   std::lock_guard<std::mutex> lock(mu);
   cudaFuncAttributes fa;

@@ -71,7 +71,8 @@ typedef enum ts_tenure { TS_TENURE_REF = 0, TS_TENURE_FIXED = 1 } ts_tenure;
  *   once for all 32 rows (32-bit keys only; 64-bit keys use TS_PASS_ROWS).
  * TS_PASS_ROWS: a few rows per tile, each pair looked up in its row's staged
  *   structure (fewer, cheaper tiles: small instances).
- * TS_PASS_AUTO: TILE from 2^22 swap pairs per iteration up, else ROWS. */
+ * TS_PASS_AUTO: TILE from 2^22 swap pairs per iteration up (CSR with
+ *   MDP or a negative weight: ROWS), else ROWS. */
 typedef enum ts_pass { TS_PASS_AUTO = 0, TS_PASS_TILE = 1, TS_PASS_ROWS = 2 } ts_pass;
 
 typedef struct ts_graph ts_graph;
