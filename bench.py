@@ -173,32 +173,44 @@ def issue_fraction(warp_inst: float, seconds: float, sm_mhz: float) -> float:
     return warp_inst / seconds / (148 * 4 * sm_mhz * 1e6)
 
 
-def cpu_baseline_sample(wl, problem, m, budget_s: float = 12.0):
-    """The oracle (exact restatement of the reference loop) on the host cores,
-    over a bounded row sample of one iteration's pair sweep."""
+def oracle_iterations(wl, problem, m, warm: int, k: int, threads: int, tenure: int):
+    """Seconds the oracle (the reference loop restated, int64) takes for k
+    whole tabu iterations (sweep + ArgMax + move) after `warm` iterations from
+    the seeded start: runs of warm and warm + k iterations, differenced, so
+    the start state's cost cancels."""
     from oracle import oracle as O
-    n = wl["n"]
     op = O.MDP if problem == 0 else O.MAXBS
-    g = O.Graph(n, wl["u"], wl["v"], wl["w"], drop_self_loops=problem == 0)
+    g = O.Graph(wl["n"], wl["u"], wl["v"], wl["w"], drop_self_loops=problem == 0)
+    kw = dict(m=m if problem == 0 else 0, tenure_policy=O.TENURE_FIXED, tenure=tenure, piter=500, gamma=150,
+              seed=1, threads=threads)
+    t0 = time.time()
+    O.run(g, op, max_iter=warm, **kw)
+    t_w = time.time() - t0
+    t0 = time.time()
+    r = O.run(g, op, max_iter=warm + k, **kw)
+    t_wk = time.time() - t0
+    assert r.iterations == warm + k
+    return max(t_wk - t_w, 1e-9)
+
+
+def cpu_baseline_sample(wl, problem, m, iters: int = 12):
+    """The oracle on all host cores: whole iterations of the same solve."""
+    from oracle import oracle as O
     threads = O.max_threads()
-    rows = min(m, max(threads, 64))
-    t, pairs, _, _ = O.sweep_sample(g, op, m=m, rows=rows, seed=1, threads=threads)
-    # grow the sample to the time budget: more rows, then more sweeps
-    sweeps = 2
-    if t > 0:
-        per_row = t / rows
-        rows = int(min(m, max(rows, budget_s / per_row / 2)))
-        sweeps = int(max(2, min(1000, budget_s / max(per_row * rows, 1e-6))))
-        t, pairs, _, _ = O.sweep_sample(g, op, m=m, rows=rows, sweeps=sweeps, seed=1, threads=threads)
-    return {"value": pairs / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"oracle OpenMP sweep of the start state: {rows} of {m} rows x {n - m} columns, "
-                      f"{sweeps} sweeps ({pairs:.3g} pairs, {t:.1f} s)"}
+    n = wl["n"]
+    P = m * (n - m)
+    dt = oracle_iterations(wl, problem, m, 2, iters, threads, wl["tenure"])
+    return {"value": P * iters / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle (OpenMP over row blocks): tabu iterations 3-{2 + iters} of the seeded solve, "
+                      f"{P:.3g} pairs each ({dt:.1f} s)"}
 
 
 def run_reference(args):
     """--impl reference: the reference loop restated on the host cores (the
     reference has no CPU implementation and its CUDA build cannot index this
-    instance's 2.5e9 pairs in int32)."""
+    instance's 2.5e9 pairs in int32): each step one whole tabu iteration
+    (all-pairs sweep, ArgMax, move) of the default workload's seeded solve,
+    after `warmup` iterations, with all host threads."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -206,29 +218,19 @@ def run_reference(args):
     wl = build_workload()
     n = wl["n"]
     m = n // 2
-    g = O.Graph(n, wl["u"], wl["v"], wl["w"], drop_self_loops=False)
+    P = m * (n - m)
     threads = O.max_threads()
-    # size one step so that warmup + steps stay within ~2.5 minutes
-    t1, p1, _, _ = O.sweep_sample(g, O.MAXBS, rows=max(threads, 64), seed=1, threads=threads)
-    per_row = t1 / max(threads, 64)
-    budget = 150.0 / max(1, args.steps + args.warmup)
-    rows = int(max(1, min(m, budget / max(per_row, 1e-9))))
-    for _ in range(args.warmup):
-        O.sweep_sample(g, O.MAXBS, rows=rows, seed=1, threads=threads)
-    tot_t, tot_p = 0.0, 0
-    for _ in range(args.steps):
-        t, p, _, _ = O.sweep_sample(g, O.MAXBS, rows=rows, seed=1, threads=threads)
-        tot_t += t
-        tot_p += p
-    value = tot_p / tot_t
+    dt = oracle_iterations(wl, 1, m, args.warmup, args.steps, threads, wl["tenure"])
+    value = P * args.steps / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded conflict-style graph)",
-        "config": {"workload": WORKLOAD, "sample_rows_per_step": rows, "rows": m, "columns": n - m},
+        "config": {"workload": WORKLOAD, "n": n, "m": m, "pairs_per_iter": P},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"each step: oracle sweep of {rows} of {m} rows x {n - m} columns"},
+                         "sample": f"tabu iterations {args.warmup + 1}-{args.warmup + args.steps} of the seeded "
+                                   "solve, whole iterations"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -347,7 +349,8 @@ def run_ours(args):
         tot_ms += ms
         avg_s = ms / 1e3 / args.steps
         per[k] = {"iters_per_s": 1.0 / avg_s, "swap_gains_per_s": P / avg_s, "ms_per_iter": ms / args.steps,
-                  "bytes_per_iter": bytes_per_iter[k], "achieved_gbs": bytes_per_iter[k] / avg_s / 1e9}
+                  "bytes_per_iter": bytes_per_iter[k], "achieved_gbs": bytes_per_iter[k] / avg_s / 1e9,
+                  "grid": solver_grid[k]}
     t_max_ms, value = whole_job_value(tot_ms, ws, P * len(kinds) * args.steps, dev)
 
     peak, peak_src = measured_peaks()
@@ -388,6 +391,7 @@ def run_ours(args):
         e2e = None if args.no_extras else run_e2e(T, torch, wl, kinds, args, seed, problem, m)
         cpu = None if args.no_extras else cpu_baseline_sample(wl, problem, m)
         batched = None if (args.no_extras or args.no_batched) else run_batched(T, torch, dev, args)
+        served = None if (args.no_extras or args.no_served) else run_served_sweep(T, torch, args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps, "higher_is_better": True,
@@ -405,6 +409,7 @@ def run_ours(args):
             "configs": configs,
             "reference_cuda": ref_cuda,
             "batched": batched,
+            "served": served,
             "gpu_launches": len(kinds) * args.steps,
             "clocks": csum,
             "wall_s_timed_region": wall,
@@ -738,6 +743,100 @@ def run_batched(T, torch, dev, args):
     }
 
 
+def _serve_once(T, reqs, arrivals, round_ms):
+    """Submits reqs[i] at arrivals[i] (seconds from the start) to a fresh
+    server and collects every completion; returns (span_s, latencies_s,
+    results, stats)."""
+    srv = T.Server(round_ms=round_ms)
+    got, tickets = {}, []
+    t0 = srv.now()
+    k = 0
+    while k < len(reqs) or len(got) < len(reqs):
+        now = srv.now() - t0
+        while k < len(reqs) and arrivals[k] <= now:
+            r = reqs[k]
+            mdp = r["problem"] == "mdp"
+            tickets.append(srv.submit(r["n"], r["u"], r["v"], r["w"], T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS,
+                                      kind="csr", m=r["m"] if mdp else 0, max_iter=r["iters"],
+                                      tenure_policy=T.TENURE_FIXED, tenure=r["tenure"], seed=r["seed"]))
+            k += 1
+        for d in srv.poll(wait_ms=1 if k < len(reqs) else 20):
+            got[d.ticket] = d
+    st = srv.stats()
+    srv.close()
+    lat = np.array([got[tk].done_s - got[tk].submit_s for tk in tickets])
+    span = max(got[tk].done_s for tk in tickets) - t0
+    return span, lat, [got[tk] for tk in tickets], st
+
+
+def run_served_sweep(T, torch, args):
+    """Served form (config 5) at three offered loads, bounded: a pool of
+    `served_requests` requests drawn as config 5 (70% MDP Chung-Lu, m = n/100,
+    tenure 100; 30% Max Bisection conflict graphs, tenure 50; n log-uniform in
+    [1e3, n_hi]; budgets U[1000, 10000]).  Capacity = requests / makespan when
+    all arrive at once; then open-loop Poisson arrivals at 0.5x and 1x that
+    capacity.  Beside each run, the plain one-at-a-time loop: the same requests
+    each run alone (graph build + ts_solver_*, their measured service times)
+    and queued FIFO at the same arrival times.  Every served result must equal
+    its alone result."""
+    t_gen = time.time()
+    reqs = T.gen.config5_requests(args.served_requests, n_hi=args.served_n_hi)
+    t_gen = time.time() - t_gen
+    service, alone = [], []
+    for r in reqs:
+        mdp = r["problem"] == "mdp"
+        torch.cuda.synchronize()
+        a = time.time()
+        g = T.Graph(r["n"], r["u"], r["v"], r["w"], "csr", drop_self_loops=mdp)
+        sv = T.Solver(g, T.PROBLEM_MDP if mdp else T.PROBLEM_MAXBS, m=r["m"] if mdp else 0, max_iter=r["iters"],
+                      tenure_policy=T.TENURE_FIXED, tenure=r["tenure"], seed=r["seed"])
+        sv.init(None)
+        sv.step(r["iters"])
+        alone.append(sv.result())
+        sv.close()
+        g.close()
+        service.append(time.time() - a)
+    pct = lambda x, q: float(np.percentile(x, q))
+
+    def summary(span, lat, res, st, arrivals):
+        ok = all(d.result is not None and (d.result.best, d.result.best_true, d.result.iterations,
+                                           d.result.evaluations) == (a.best, a.best_true, a.iterations, a.evaluations)
+                 and bool(np.array_equal(d.result.best_sol, a.best_sol)) for d, a in zip(res, alone))
+        fin, plain_lat = 0.0, []
+        for arr, sv_t in zip(arrivals, service):
+            fin = max(arr, fin) + sv_t
+            plain_lat.append(fin - arr)
+        plain_lat = np.array(plain_lat)
+        return {"solves_per_s": len(reqs) / span, "span_s": span,
+                "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": float(lat.max())},
+                "plain_one_at_a_time": {"solves_per_s": len(reqs) / fin, "span_s": fin,
+                                        "latency_s": {"p50": pct(plain_lat, 50), "p95": pct(plain_lat, 95),
+                                                      "p99": pct(plain_lat, 99), "max": float(plain_lat.max())}},
+                "identical_to_alone": bool(ok), "rounds": st.rounds,
+                "executors": {e: sum(1 for d in res if d.executor == e) for e in ("packed", "plain")}}
+
+    out = {"workload": f"config5 pool: {len(reqs)} requests, 70% MDP Chung-Lu (m=n/100, tenure 100) / 30% MaxBS "
+                       f"conflict (tenure 50), n log-uniform [1000,{args.served_n_hi}], budgets U[1000,10000], "
+                       "structure csr",
+           "n_range": [min(r["n"] for r in reqs), max(r["n"] for r in reqs)], "generation_s": t_gen,
+           "alone_service_s_total": float(sum(service))}
+    zero = [0.0] * len(reqs)
+    span, lat, res, st = _serve_once(T, reqs, zero, args.round_ms)
+    cap = len(reqs) / span
+    out["capacity_solves_per_s"] = cap
+    out["saturation"] = summary(span, lat, res, st, zero)
+    rng = np.random.default_rng(55)
+    for f in (0.5, 1.0):
+        arrivals = list(np.cumsum(rng.exponential(1.0 / (f * cap), size=len(reqs))))
+        span, lat, res, st = _serve_once(T, reqs, arrivals, args.round_ms)
+        d = summary(span, lat, res, st, arrivals)
+        d["offered_per_s"] = f * cap
+        out[f"load_{f:g}x"] = d
+    out["served_vs_plain_at_saturation"] = out["saturation"]["solves_per_s"] / \
+        out["saturation"]["plain_one_at_a_time"]["solves_per_s"]
+    return out
+
+
 def run_served(args):
     """Served workload (config 5): open-loop Poisson arrivals at `rate`/s for
     `duration` s; 70% MDP (Chung-Lu graphs) / 30% Max Bisection (conflict
@@ -849,6 +948,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="config2/config3 at another size (profiling cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, CPU-baseline and batched legs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (config 4) leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served (config 5) load sweep")
+    ap.add_argument("--served-requests", type=int, default=24, help="served sweep: requests in the pool")
     ap.add_argument("--sweep", choices=["auto", "tile", "rows"], default="auto",
                     help="pair sweep of the main leg's solvers (ts_pass; auto picks by size)")
     ap.add_argument("--no-configs", action="store_true",
