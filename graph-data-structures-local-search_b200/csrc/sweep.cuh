@@ -1180,36 +1180,48 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
       const KeyT t = s_rv[r];
       const bool rt = s_rtab[r] != 0;
       // Only a thread whose own maximum of this row equals the target swept a
-      // matching column, so only such threads (usually one) rescan their own
-      // columns, in the order they swept them.
+      // matching column, so only such threads (usually one) hold the answer.
+      // Each one's columns (pass-major, then the four of a pass: ascending)
+      // are rescanned by its whole warp, one column per lane, 32 at a time,
+      // so the loads of a round are all in flight together; the lowest
+      // matching lane of the first round with a match is that thread's
+      // lowest matching column.
       KeyT mine = Lim::none;
 #pragma unroll
       for (int rr = 0; rr < R; rr++)
         if (rr == r) mine = best[rr];
       uint32_t cmin = 0xffffffffu;
-      if (mine == target) {
-        for (int pass = 0; pass < passes && cmin == 0xffffffffu; pass++) {
-          const int32_t cb = c0 + (pass * TPB + tid) * kColsPerLane;
-          if (cb >= c_end) break;
-          for (int q = 0; q < kColsPerLane; q++) {
-            const int32_t c = cb + q;
-            if (c >= c_end) break;
+      unsigned who = __ballot_sync(0xffffffffu, mine == target);
+      const int32_t ncols = passes * kColsPerLane;
+      while (who) {
+        const int32_t tt = (tid & ~31) + (__ffs(who) - 1);
+        who &= who - 1;
+        for (int32_t j0 = 0; j0 < ncols; j0 += 32) {
+          const int32_t j = j0 + lane;
+          const int32_t c = c0 + ((j / kColsPerLane) * TPB + tt) * kColsPerLane + (j % kColsPerLane);
+          bool hit = false;
+          if (j < ncols && c < c_end) {
             int32_t w = 0;
+            bool skip = false;
             if (ST == S_CSR) {
               // adjacent pairs are matched below from the row's entries; when
               // not masked (MaxBS, w >= 0) an adjacent pair's w-free gain never
               // exceeds its exact gain, so it cannot equal the row maximum alone.
-              if (masked && ((s_mask[c - c0] >> r) & 1u)) continue;
+              skip = masked && ((s_mask[c - c0] >> r) & 1u);
             } else if (ST == S_WSWAP) {
               w = w_get<PERSIST>(s, (long long)(r0 + r) * s.ldc + c);
             } else {
               w = staged_lookup<ST>(s_desc[r], ld_st<PERSIST>(s.sol_out + c));
             }
             const KeyT x = pair_gain<PROB, KeyT>(t, ld_st<PERSIST>(s.vg_out + c), w);
-            if (x == target && allowed(rt, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D)) {
-              cmin = (uint32_t)c;
-              break;
-            }
+            hit = !skip && x == target &&
+                  allowed(rt, ld_st<PERSIST>(s.tab_out + c) > iter, (long long)x, (long long)D);
+          }
+          const unsigned hb = __ballot_sync(0xffffffffu, hit);
+          if (hb) {
+            const uint32_t cc = (uint32_t)__shfl_sync(0xffffffffu, c, __ffs(hb) - 1);
+            cmin = cc < cmin ? cc : cmin;
+            break;
           }
         }
       }
