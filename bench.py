@@ -689,9 +689,11 @@ def run_batched(T, torch, dev, args):
     # device-timed replay
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
+    torch.cuda.nvtx.range_push("config4 replay")  # ncu --nvtx --nvtx-include "config4 replay/"
     ev0.record(stream)
     b.launch()
     ev1.record(stream)
+    torch.cuda.nvtx.range_pop()
     b.sync()
     torch.cuda.synchronize(dev)
     dev_s = ev0.elapsed_time(ev1) / 1e3

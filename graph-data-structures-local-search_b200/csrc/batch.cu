@@ -398,6 +398,7 @@ extern "C" {
 
 ts_status ts_batch_create(const ts_batch_job* jobs, int32_t count, const ts_batch_opts* opts,
                           void* stream, ts_batch** out) {
+  tsb::TraceRange tr_("ts_batch_create");
   if (!out) { set_error("ts_batch_create: out is NULL"); return TS_ERR_INVALID_ARG; }
   *out = nullptr;
   if (count < 1 || !jobs) { set_error("ts_batch_create: need count >= 1 jobs"); return TS_ERR_INVALID_ARG; }
@@ -614,6 +615,7 @@ ts_status ts_batch_create(const ts_batch_job* jobs, int32_t count, const ts_batc
 }
 
 ts_status ts_batch_launch(ts_batch* b) {
+  tsb::TraceRange tr_("ts_batch_launch");
   if (!b) { set_error("ts_batch_launch: NULL batch"); return TS_ERR_INVALID_ARG; }
   TS_CUDA(cudaSetDevice(b->device));
   TS_CUDA(cudaGraphLaunch(b->exec, b->stream));
@@ -621,6 +623,7 @@ ts_status ts_batch_launch(ts_batch* b) {
 }
 
 ts_status ts_batch_sync(ts_batch* b) {
+  tsb::TraceRange tr_("ts_batch_sync");
   if (!b) { set_error("ts_batch_sync: NULL batch"); return TS_ERR_INVALID_ARG; }
   TS_CUDA(cudaSetDevice(b->device));
   TS_CUDA(cudaStreamSynchronize(b->stream));
@@ -628,6 +631,7 @@ ts_status ts_batch_sync(ts_batch* b) {
 }
 
 ts_status ts_batch_results(ts_batch* b, ts_result* out, int32_t* best_sols) {
+  tsb::TraceRange tr_("ts_batch_results");
   if (!b) { set_error("ts_batch_results: NULL batch"); return TS_ERR_INVALID_ARG; }
   TS_CUDA(cudaSetDevice(b->device));
   std::vector<BatchResultDev> r(b->count);

@@ -189,6 +189,8 @@ struct FastSh {
   uint32_t rescan;   // rows swept again alone
   uint32_t group;    // rows of the current group
   uint32_t done_rows;
+  int32_t ngroups;   // groups formed so far (this tile's work units, in order)
+  int32_t gsel;      // the current group is this CTA's (its slice of the tile)
   int32_t ok;        // bulk copies completed
 };
 
@@ -634,9 +636,14 @@ __device__ void fast_row_sweep(const DevSolver<int32_t>& s, FastSh& sh, int r, i
 
 // The fast pass of one tile (32-bit keys, mode 0).  (out_key, out_idx) valid
 // in thread 0; (LLONG_MIN, LLONG_MAX) when the tile has no allowed pair.
+// Work units of a tile: its groups, then its heavy rows, in order.  With
+// nslices > 1 several CTAs share the tile: slice k takes the units whose
+// index is k mod nslices (every slice forms the same groups from the rows'
+// degrees), so a tile whose rows hold far more entries than one index is
+// spread over CTAs instead of running its units one after another.
 template <int PROB, int ST, bool PERSIST>
 __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long long iter, long long D64, int rb,
-                          int ch, long long& out_key, long long& out_idx) {
+                          int ch, long long& out_key, long long& out_idx, int slice = 0, int nslices = 1) {
   __shared__ FastSh sh;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -664,7 +671,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
     sh.rcap[tid] = (int32_t)(hb1 - hb);
     sh.best[tid] = 0ull;
   }
-  if (tid == 0) sh.done_rows = 0u;
+  if (tid == 0) { sh.done_rows = 0u; sh.ngroups = 0; }
   __syncthreads();
 
   const uint32_t all_rows = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
@@ -689,6 +696,8 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
       }
       sh.group = grp;
       sh.done_rows |= grp;
+      sh.gsel = grp != 0u && sh.ngroups % nslices == slice;
+      if (grp != 0u) sh.ngroups++;
       sh.qn = 0;
       sh.tqn = 0;
       // Hub rows are adjacent to every top column (hubs are adjacent to each
@@ -698,7 +707,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
       // under-estimate adjacent pairs.)
       int32_t nt = 0;
       uint32_t tm = 0u;
-      if (ST != S_CSR || masked_csr) {
+      if (sh.gsel && (ST != S_CSR || masked_csr)) {
         for (int t = 0; t < kTrack; t++) {
           int best_r = -1;
           for (int r = 0; r < nr; r++)
@@ -719,6 +728,10 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
     __syncthreads();
     const uint32_t grp = sh.group;
     if (grp == 0u) break;
+    if (!sh.gsel) {  // another slice's group
+      __syncthreads();
+      continue;
+    }
 
     // ---------------- index of the group
     uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw);  // CSR: rows adjacent to each column
@@ -1059,9 +1072,11 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
     uint32_t hv = all_rows & ~sh.done_rows;
     uint32_t* cbits = reinterpret_cast<uint32_t*>(smem_raw);  // the index is no longer needed
     const int32_t cw = (c_end - c0 + 31) >> 5;
+    int32_t unit = sh.ngroups;  // heavy rows follow the groups in the unit order
     while (hv) {
       const int r = __ffs(hv) - 1;
       hv &= hv - 1;
+      if (unit++ % nslices != slice) continue;  // another slice's row
       const int32_t u = sh.ru[r], rv = sh.rv[r];
       for (int32_t q = tid; q < cw; q += T) cbits[q] = 0u;
       __syncthreads();

@@ -471,12 +471,14 @@ const char* ts_struct_name(int32_t kind) {
 ts_status ts_graph_create_device(int32_t n, int64_t num_edges, const int32_t* d_u, const int32_t* d_v,
                                  const int32_t* d_w, int32_t kind, int32_t drop_self_loops,
                                  void* stream, ts_graph** out) {
+  tsb::TraceRange tr_("ts_graph_create_device");
   return make_graph(n, num_edges, d_u, d_v, d_w, kind, drop_self_loops, stream, out);
 }
 
 ts_status ts_graph_create(int32_t n, int64_t num_edges, const int32_t* u, const int32_t* v,
                           const int32_t* w, int32_t kind, int32_t drop_self_loops, void* stream,
                           ts_graph** out) {
+  tsb::TraceRange tr_("ts_graph_create");
   if (!out) { set_error("ts_graph_create: out is NULL"); return TS_ERR_INVALID_ARG; }
   *out = nullptr;
   if (num_edges < 0 || (num_edges > 0 && (!u || !v || !w))) {
@@ -531,6 +533,7 @@ ts_status ts_graph_destroy(ts_graph* g) {
 
 ts_status ts_lookup(const ts_graph* g, int64_t count, const int32_t* d_u, const int32_t* d_v,
                     int32_t* d_w_out) {
+  tsb::TraceRange tr_("ts_lookup");
   if (!g || count < 0 || (count > 0 && (!d_u || !d_v || !d_w_out))) {
     set_error("ts_lookup: bad argument");
     return TS_ERR_INVALID_ARG;

@@ -407,6 +407,7 @@ void ts_server::admit() {
 }
 
 void ts_server::round() {
+  TraceRange tr_("ts_server round");
   const double round_s = opts.round_ms * 1e-3;
   const double t_round = now_s(t0);
   // Plain solves get the iterations that fill the round at their measured
@@ -657,6 +658,7 @@ ts_status ts_server_create(const ts_server_opts* opts, ts_server** out) {
 }
 
 ts_status ts_server_submit(ts_server* s, const ts_request* q, int64_t* ticket) {
+  tsb::TraceRange tr_("ts_server_submit");
   if (!s || !q || (q->num_edges > 0 && (!q->u || !q->v || !q->w)) || q->num_edges < 0) {
     set_error("ts_server_submit: bad arguments");
     return TS_ERR_INVALID_ARG;
@@ -701,6 +703,7 @@ ts_status ts_server_submit(ts_server* s, const ts_request* q, int64_t* ticket) {
 }
 
 ts_status ts_server_poll(ts_server* s, ts_served* out, int32_t cap, int32_t* n_out, int32_t wait_ms) {
+  tsb::TraceRange tr_("ts_server_poll");
   if (!s || (cap > 0 && !out)) { set_error("ts_server_poll: bad arguments"); return TS_ERR_INVALID_ARG; }
   std::unique_lock<std::mutex> lk(s->mu);
   if (s->done.empty() && wait_ms > 0)

@@ -639,12 +639,18 @@ __device__ void decide_apply(const DevGraph& g, const DevSolver<KeyT>& s, int mo
 template <int PROB, int ST, class KeyT, bool PERSIST, bool W16K = false>
 __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode, long long iter,
                           long long D64, int rb, int ch, long long& out_key, long long& out_idx,
-                          TailShared& sh, long long floor_key = LLONG_MIN) {
+                          TailShared& sh, long long floor_key = LLONG_MIN, int slice = 0,
+                          int nslices = 1) {
   if constexpr (std::is_same<KeyT, int32_t>::value && ST != S_WSWAP) {
     if (mode == 0 && s.fast) {
-      tile_fast<PROB, ST, PERSIST>(g, s, iter, D64, rb, ch, out_key, out_idx);
+      tile_fast<PROB, ST, PERSIST>(g, s, iter, D64, rb, ch, out_key, out_idx, slice, nslices);
       return;
     }
+  }
+  if (slice != 0) {  // the other passes take a tile in one CTA: slice 0's
+    out_key = LLONG_MIN;
+    out_idx = LLONG_MAX;
+    return;
   }
   constexpr int R = Rows<ST>::R;
   constexpr int TPB = TpbOf<ST, PERSIST>::v;
@@ -1268,6 +1274,12 @@ template <int PROB, int ST, class KeyT> struct IterMinBlocks {
 template <int PROB, int ST, class KeyT, bool W16K = false>
 __global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT>::v))
 iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
+  // Small grids are launched with programmatic stream serialization: the
+  // previous iteration's grid may still be finishing.  Wait for it (all of
+  // its memory visible), then let the next iteration's grid be scheduled.
+  // (Both are no-ops for a grid launched without that attribute.)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   DevState* st = s.st;
   if (st->done || st->iter >= st->target) return;
   const int mode = st->mode;
@@ -1276,8 +1288,11 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __shared__ TailShared sh;
   __shared__ int32_t s_last;
   long long k, i;
-  tile_eval<PROB, ST, KeyT, false, W16K>(g, s, mode, iter, D64, blockIdx.x / s.n_chunks,
-                                   blockIdx.x % s.n_chunks, k, i, sh);
+  // CTA -> (tile, slice): the slices of a tile are adjacent CTAs
+  const int ns = s.n_slices > 1 ? s.n_slices : 1;
+  const int tile = (int)blockIdx.x / ns, slice = (int)blockIdx.x % ns;
+  tile_eval<PROB, ST, KeyT, false, W16K>(g, s, mode, iter, D64, tile / s.n_chunks, tile % s.n_chunks, k, i, sh,
+                                         LLONG_MIN, slice, ns);
   if (threadIdx.x == 0) {
     CtaRec rec;
     rec.key = k;

@@ -8,10 +8,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "ts_b200.h"
 #include "ts_internal.cuh"
 
 namespace tsb {
+
+// Names the span of a C-ABI call on a profiler's timeline (NVTX range: ncu
+// --nvtx filters, Nsight Systems); a no-op unless a tool is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 // Thread-local message of the last failing call.
 void set_error(const std::string& msg);

@@ -101,6 +101,9 @@ struct DevSolver {
   int32_t tile_rows;
   int32_t fast;
   int32_t fast_ecap;
+  // Plain kernel, fast pass: CTAs per tile (each takes every n_slices-th of
+  // the tile's work units); 1 (or 0: unset) = one CTA per tile.
+  int32_t n_slices;
   // WSwap: 1 when the matrix holds 16-bit weights (every |w| <= 32767), read
   // through W as int16_t; 0: 32-bit.
   int32_t w16;

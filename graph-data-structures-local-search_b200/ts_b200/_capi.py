@@ -56,7 +56,8 @@ class SolverInfo(ctypes.Structure):
     _fields_ = [
         ("grid", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("chunk_cols", ctypes.c_int32),
         ("n_chunks", ctypes.c_int32), ("threads", ctypes.c_int32), ("dyn_smem_bytes", ctypes.c_int32),
-        ("key_bytes", ctypes.c_int32), ("w_bytes", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
+        ("key_bytes", ctypes.c_int32), ("w_bytes", ctypes.c_int32), ("slices", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 

@@ -100,7 +100,8 @@ typedef struct ts_solver_info {
   int32_t dyn_smem_bytes; /* dynamic shared memory per CTA */
   int32_t key_bytes;      /* 4: 32-bit pair keys and contributions, 8: 64-bit */
   int32_t w_bytes;        /* WSwap: bytes per matrix element (2 or 4); 0 otherwise */
-  int32_t reserved[8];
+  int32_t slices;         /* CTAs per tile (grid = row blocks x n_chunks x slices) */
+  int32_t reserved[7];
 } ts_solver_info;
 
 typedef struct ts_params {
@@ -206,8 +207,8 @@ ts_status ts_solver_set_perturbations(ts_solver* s, const int64_t* draws, int64_
  * Blocks until they are done; *done_iters (may be NULL) = iterations applied
  * by this call. */
 ts_status ts_solver_step(ts_solver* s, int64_t k, int64_t* done_iters);
-/* Asynchronous stepping, for callers that overlap work, bracket iterations
- * with their own CUDA events, or capture them in a CUDA graph:
+/* Asynchronous stepping, for callers that overlap work or bracket iterations
+ * with their own CUDA events:
  *   ts_solver_prepare(s, k, &adm)  synchronises, admits adm <= k iterations
  *       (bounded by max_iter; MaxBS also by its staged perturbation draws,
  *       about 62*piter per call) and stages what they need;
@@ -382,8 +383,7 @@ ts_status ts_server_destroy(ts_server* s);
  * n above TS_NOALLOC_MAX_N is rejected (TS_ERR_INVALID_ARG).  Work runs on
  * `stream` without synchronising, in the CUDA context current on the calling
  * thread (the device's primary context if none is).  The first call in each
- * context looks the scratch address up; it should come before any stream
- * capture.  All calls share the scratch, so calls that overlap on the GPU
+ * context looks the scratch address up.  All calls share the scratch, so calls that overlap on the GPU
  * (other streams or host threads) race on it.  Cost: one binary search of a
  * global CSR row per pair, roughly P / 1e10 s for P = m*(n-m) pairs. */
 #define TS_NOALLOC_MAX_N 262144

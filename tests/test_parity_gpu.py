@@ -311,3 +311,47 @@ def test_caller_supplied_perturbation_stream(gpu, kind):
     finally:
         s.close()
         g.close()
+
+
+def hub_graph(n, seed, hubs=((24, 5000), (24, 1500)), base_deg=10):
+    """Erdos-Renyi background plus groups of hub vertices joined to random
+    vertices: (count, degree) per group.  The 32 largest degrees exceed one
+    tile index many times over, so the tile pass splits tiles over CTAs."""
+    rng = np.random.default_rng(seed)
+    u, v, w, _ = T.gen.erdos_renyi(n, base_deg, seed)
+    us, vs = [u], [v]
+    ids = rng.permutation(n)
+    k = 0
+    for count, deg in hubs:
+        for h in ids[k:k + count]:
+            nb = rng.choice(n, size=deg, replace=False)
+            nb = nb[nb != h]
+            us.append(np.full(len(nb), h, np.int32))
+            vs.append(nb.astype(np.int32))
+        k += count
+    u = np.concatenate(us).astype(np.int32)
+    v = np.concatenate(vs).astype(np.int32)
+    w = rng.integers(1, 1000, size=len(u)).astype(np.int32)
+    return u, v, w
+
+
+@pytest.mark.parametrize("kind", ["hash", "csr-bitset", "csr-bb", "csr-bitset-bb"])
+@pytest.mark.parametrize("problem", [T.PROBLEM_MDP, T.PROBLEM_MAXBS], ids=["mdp", "maxbs"])
+def test_tile_slices_with_hub_rows(gpu, kind, problem):
+    # hubs of degree 5,000 (more entries than a tile index holds: heavy rows)
+    # and 1,500; MDP pulls them into the solution within a few iterations
+    n = 6000
+    u, v, w = hub_graph(n, 17)
+    mdp = problem == T.PROBLEM_MDP
+    m = 600 if mdp else 0
+    g = T.Graph(n, u, v, w, kind, drop_self_loops=mdp)
+    s = T.Solver(g, problem, m=m, max_iter=10, tenure_policy=T.TENURE_FIXED, tenure=20, seed=1,
+                 sweep=T.PASS_TILE)
+    try:
+        info = s.info()
+        assert info.slices > 1 and info.grid % info.slices == 0
+    finally:
+        s.close()
+        g.close()
+    compare_run(problem, kind, n, u, v, w, m=m, iters=200 if mdp else 100, tenure_policy=T.TENURE_FIXED,
+                tenure=20, sweep=T.PASS_TILE, step_chunks=(37, None))
