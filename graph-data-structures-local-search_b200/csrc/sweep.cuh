@@ -469,16 +469,32 @@ __device__ long long apply_swap(const DevGraph& g, const DevSolver<KeyT>& s, int
     // returning the CSR lookup's w(u, v).  Plain stores: every element is
     // written by one entry, after the barrier that ends the clearing.
     __syncthreads();
-    for (int32_t k = threadIdx.x; k < total; k += blockDim.x) {
-      const bool from_u = k < nu;
-      const long long at = from_u ? su + k : sv + (k - nu);
-      const long long rs = from_u ? su : sv;
-      const int2 e = g.adj[at];
-      if (e.x == u || e.x == v) continue;
-      if (at != rs && g.adj[at - 1].x == e.x) continue;
-      const int32_t p = s.pos[e.x];
-      if (!from_u && p >= m) w_set(s, (long long)iu * s.ldc + (p - m), e.y);
-      if (from_u && p < m) w_set(s, (long long)p * s.ldc + jv, e.y);
+    for (int32_t base = 0; base < total; base += kApplyBatch * (int32_t)blockDim.x) {
+      int2 e[kApplyBatch];
+      int32_t prev[kApplyBatch], pz[kApplyBatch];
+#pragma unroll
+      for (int j = 0; j < kApplyBatch; j++) {  // the batch's loads before any use
+        const int32_t k = base + j * (int32_t)blockDim.x + (int32_t)threadIdx.x;
+        const bool from_u = k < nu;
+        const long long at = from_u ? su + k : sv + (k - nu);
+        e[j] = make_int2(-1, 0);
+        prev[j] = -1;
+        if (k < total) {
+          e[j] = g.adj[at];
+          if (at != (from_u ? su : sv)) prev[j] = g.adj[at - 1].x;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kApplyBatch; j++) pz[j] = e[j].x >= 0 ? s.pos[e[j].x] : 0;
+#pragma unroll
+      for (int j = 0; j < kApplyBatch; j++) {
+        const int32_t k = base + j * (int32_t)blockDim.x + (int32_t)threadIdx.x;
+        if (k >= total || e[j].x == u || e[j].x == v || prev[j] == e[j].x) continue;
+        const bool from_u = k < nu;
+        const int32_t p = pz[j];
+        if (!from_u && p >= m) w_set(s, (long long)iu * s.ldc + (p - m), e[j].y);
+        if (from_u && p < m) w_set(s, (long long)p * s.ldc + jv, e[j].y);
+      }
     }
   }
   __syncthreads();
@@ -1265,14 +1281,19 @@ __device__ void tile_eval(const DevGraph& g, const DevSolver<KeyT>& s, int mode,
 // Minimum resident CTAs per SM the plain kernel is compiled for (0: left to
 // the compiler).  The 512-thread index structures are held to two CTAs per SM
 // (at most 64 registers): their sweep hides latency with warps.  WSwap is
-// left to the compiler: holding it to 64-80 registers spilled its 16 rows of
-// packed matrix loads.
-template <int PROB, int ST, class KeyT> struct IterMinBlocks {
-  static constexpr int v = (ST == S_CSR || ST == S_WSWAP) ? 0 : 2;
+// left to the compiler (holding its 32-bit matrix kernel to 64-80 registers
+// spilled its 16 rows of packed matrix loads), except the Max Bisection
+// kernel for the 16-bit matrix: held to four CTAs per SM (64 registers) it
+// keeps more matrix loads in flight and streams the n = 100,000 matrix at
+// 0.81 of measured HBM instead of 0.73.  The MDP one lost there (0.60 instead
+// of 0.65 on the Chung-Lu n = 200,000 case) and stays at three.
+template <int PROB, int ST, class KeyT, bool W16K = false> struct IterMinBlocks {
+  static constexpr int v = (ST == S_WSWAP && W16K && PROB == P_MAXBS) ? 4
+                           : (ST == S_CSR || ST == S_WSWAP) ? 0 : 2;
 };
 
 template <int PROB, int ST, class KeyT, bool W16K = false>
-__global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT>::v))
+__global__ void __launch_bounds__(Tpb<ST>::v, (IterMinBlocks<PROB, ST, KeyT, W16K>::v))
 iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   // Small grids are launched with programmatic stream serialization: the
   // previous iteration's grid may still be finishing.  Wait for it (all of
@@ -1307,8 +1328,26 @@ iter_kernel(const DevGraph g, const DevSolver<KeyT> s) {
   __threadfence();
   k = LLONG_MIN;
   i = LLONG_MAX;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-    better_rec(k, i, __ldcg(&s.recs[b].key), __ldcg(&s.recs[b].idx));
+  // Grids of more CTAs than threads: kRecBatch records per thread in flight
+  // per round (thousands of tiles are otherwise a chain of dependent L2
+  // round trips); smaller ones read one record per thread.
+  constexpr int kRecBatch = 8;
+  if ((int)gridDim.x <= (int)blockDim.x) {
+    if ((int)threadIdx.x < (int)gridDim.x)
+      better_rec(k, i, __ldcg(&s.recs[threadIdx.x].key), __ldcg(&s.recs[threadIdx.x].idx));
+  } else {
+    for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += kRecBatch * blockDim.x) {
+      longlong2 r[kRecBatch];
+#pragma unroll
+      for (int j = 0; j < kRecBatch; j++) {
+        const int b = b0 + j * (int)blockDim.x;
+        r[j] = b < (int)gridDim.x ? __ldcg(reinterpret_cast<const longlong2*>(&s.recs[b]))
+                                  : make_longlong2(LLONG_MIN, LLONG_MAX);
+      }
+#pragma unroll
+      for (int j = 0; j < kRecBatch; j++) better_rec(k, i, r[j].x, r[j].y);
+    }
+  }
   block_best(k, i, sh.red);
   decide_apply<PROB, ST, KeyT>(g, s, mode, k, i, sh);
   if (threadIdx.x == 0) st->counter = 0;
