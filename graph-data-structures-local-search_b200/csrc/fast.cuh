@@ -244,11 +244,28 @@ struct FastIndex {
   // the first entry of v, found by a linear scan (CSR+Bitset,
   // GPU-MDP-CSR-Bitset.cu edge lookup) or a lower_bound (CSR+Bitset+BB).
   __device__ __forceinline__ int32_t staged_weight(int r, int32_t v) const {
-    const int2* e = stage() + sh.soff[r] + (int32_t)(sh.rrow[r] & 1);
+    const int32_t o = (int32_t)(sh.rrow[r] & 1);
+    const int2* e = stage() + sh.soff[r] + o;
     const int32_t len = sh.rdeg[r];
     if (ST == S_BITSET) {
-      for (int32_t k = 0; k < len; k++)
-        if (e[k].x == v) return e[k].y;
+      // two entries per 16-byte load: the row's slot starts on an even entry
+      // (16 bytes), the row itself at entry o of it
+      const int4* p = reinterpret_cast<const int4*>(stage() + sh.soff[r]);
+      const int32_t end = o + len;
+      const int32_t pairs = (end + 1) >> 1;  // 16-byte words holding the row
+      int32_t j = 0;
+      for (; j + 1 < pairs; j += 2) {  // two words per trip, both loads first
+        const int4 q0 = p[j], q1 = p[j + 1];
+        if (q0.x == v && 2 * j >= o) return q0.y;
+        if (q0.z == v) return q0.w;
+        if (q1.x == v) return q1.y;
+        if (q1.z == v && 2 * j + 3 < end) return q1.w;
+      }
+      if (j < pairs) {
+        const int4 q = p[j];
+        if (q.x == v && 2 * j >= o) return q.y;
+        if (q.z == v && 2 * j + 1 < end) return q.w;
+      }
       return 0;
     }
     int32_t lo = 0, n = len;
