@@ -780,7 +780,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
         int2 ej[kJ];
         bool dj[kJ];
 #pragma unroll
-        for (int j = 0; j < kJ; j++) {  // round 1: cpos and the entries
+        for (int j = 0; j < kJ; j++) {  // first loads: cpos and the entries
           const int32_t f = f0 + j * T + lane;
           rj[j] = -1;
           kj[j] = 0;
@@ -802,7 +802,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
         }
         int32_t cvj[kJ], ctj[kJ];
 #pragma unroll
-        for (int j = 0; j < kJ; j++) {  // round 2: the columns' state
+        for (int j = 0; j < kJ; j++) {  // second loads: the columns' state
           const bool in = rj[j] >= 0 && !dj[j] && cj[j] >= c0 && cj[j] < c_end;
           if (!in) rj[j] = -1;
           cvj[j] = in ? ld_st<PERSIST>(s.vg_out + cj[j]) : 0;
