@@ -181,6 +181,7 @@ struct FastSh {
   uint32_t trk_mask;
   unsigned long long trkbest[kTrack];  // packed (contribution, column) per tracked row
   int32_t tqn;                  // tabu columns queued for the warp-wide evaluation
+  int32_t lqn;                  // CSR+Bitset: hits on long rows queued for a warp-wide scan (reuses tq)
   int32_t tq[kTabuQueue];
   int32_t ntop;
   int32_t nb;        // Hash: buckets; BB: directory buckets
@@ -275,6 +276,30 @@ struct FastIndex {
       else n = half;
     }
     return (lo < len && e[lo].x == v) ? e[lo].y : 0;
+  }
+
+  // staged_weight for a whole warp (every lane passes the same r and v):
+  // the lanes read 32 of the row's 16-byte words at a time, the first
+  // matching entry in row order wins.  For rows of hundreds of entries.
+  __device__ __forceinline__ int32_t staged_weight_warp(int r, int32_t v, int lane) const {
+    const int32_t o = (int32_t)(sh.rrow[r] & 1);
+    const int4* p = reinterpret_cast<const int4*>(stage() + sh.soff[r]);
+    const int32_t end = o + sh.rdeg[r];
+    const int32_t words = (end + 1) >> 1;
+    for (int32_t j0 = 0; j0 < words; j0 += 32) {
+      const int32_t j = j0 + lane;
+      bool h0 = false, h1 = false;
+      int32_t hw = 0;
+      if (j < words) {
+        const int4 q = p[j];
+        h0 = q.x == v && 2 * j >= o;
+        h1 = q.z == v && 2 * j + 1 < end;
+        hw = h0 ? q.y : q.w;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, h0 || h1);
+      if (b) return __shfl_sync(0xffffffffu, hw, __ffs(b) - 1);
+    }
+    return 0;
   }
 
   // Calls f(r, w) for every row r of the group adjacent to v, with w(u_r, v).
@@ -717,6 +742,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
       if (grp != 0u) sh.ngroups++;
       sh.qn = 0;
       sh.tqn = 0;
+      sh.lqn = 0;
       // Hub rows are adjacent to every top column (hubs are adjacent to each
       // other), so the shared top-2 rarely serves them: the sweep tracks the
       // best free column of up to kTrack of the group's highest-degree rows.
@@ -968,15 +994,50 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
     }
 
     // ---------------- exact pairs of the adjacent columns
+    // (CSR+Bitset: a hit on a row of more than kLongScan entries is queued
+    // and scanned by a whole warp afterwards, so one thread's hub-row scans
+    // do not hold the CTA at its next barrier; the queue reuses the tabu
+    // queue's memory, free once the tabu columns are done)
     if (ST != S_CSR) {
+      constexpr int32_t kLongScan = 256;
+      if (ST == S_BITSET) __syncthreads();
       const int32_t qn = sh.qn;
       for (int32_t i = tid; i < qn; i += T) {
         const int32_t c = Q[i];
         const int32_t v = ld_st<PERSIST>(s.sol_out + c);
         const int32_t cvv = ld_st<PERSIST>(s.vg_out + c);
-        ix.for_rows(v, [&](int r, int32_t w) {
-          atomicMax(&sh.best[r], pack_kc(pair_gain<PROB, int32_t>(sh.rv[r], cvv, w), c));
-        });
+        if constexpr (ST == S_BITSET) {
+          uint32_t mk = ix.mask_of(v);
+          while (mk) {
+            const int r = __ffs(mk) - 1;
+            mk &= mk - 1;
+            if (sh.rdeg[r] > kLongScan) {
+              const int32_t at = atomicAdd(&sh.lqn, 1);
+              if (at < kTabuQueue) {
+                sh.tq[at] = (c << 5) | r;
+                continue;
+              }
+            }
+            atomicMax(&sh.best[r], pack_kc(pair_gain<PROB, int32_t>(sh.rv[r], cvv, ix.staged_weight(r, v)), c));
+          }
+        } else {
+          ix.for_rows(v, [&](int r, int32_t w) {
+            atomicMax(&sh.best[r], pack_kc(pair_gain<PROB, int32_t>(sh.rv[r], cvv, w), c));
+          });
+        }
+      }
+      if (ST == S_BITSET) {
+        __syncthreads();
+        const int32_t lqn = min(sh.lqn, kTabuQueue);
+        for (int32_t i = warp; i < lqn; i += (T >> 5)) {
+          const int32_t it = sh.tq[i];
+          const int32_t c = it >> 5;
+          const int r = it & 31;
+          const int32_t v = ld_st<PERSIST>(s.sol_out + c);
+          const int32_t cvv = ld_st<PERSIST>(s.vg_out + c);
+          const int32_t w = ix.staged_weight_warp(r, v, lane);
+          if (lane == 0) atomicMax(&sh.best[r], pack_kc(pair_gain<PROB, int32_t>(sh.rv[r], cvv, w), c));
+        }
       }
     }
 
