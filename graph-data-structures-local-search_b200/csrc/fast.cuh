@@ -1014,7 +1014,7 @@ __device__ void tile_fast(const DevGraph& g, const DevSolver<int32_t>& s, long l
             if (sh.rdeg[r] > kLongScan) {
               const int32_t at = atomicAdd(&sh.lqn, 1);
               if (at < kTabuQueue) {
-                sh.tq[at] = (c << 5) | r;
+                sh.tq[at] = (c << 5) | r;  // c < n: a bitmap that fits in HBM keeps n far below 2^26
                 continue;
               }
             }
